@@ -1,0 +1,315 @@
+"""cucm_b200 -- Python face of the B200 CuCM coder (libcucm.so, include/cucm.h).
+
+The reference (OceanCT/CuCM) exposes its hot path as host functions inside
+two CUDA programs; this module binds the C ABI that replaces them and keeps
+their names and argument meaning:
+
+  compress_batch(data, chunksize, unitlength)        compress_batch,  cucm_compress_v2.cu:990
+  decompressbatch(body, out_size, chunksize, unit)   decompressbatch, cucm_decompress_v2.cu:898
+  compress_file(in_path, out_path, ...)              compress_file,   cucm_compress_v2.cu:1151
+  decompress(in_path, out_path)                      decompress,      cucm_decompress_v2.cu:1185
+
+plus whole-buffer compress()/decompress() and a Context for repeated calls.
+Everything runs on the GPU through libcucm.so; there is no CPU fallback, and
+a missing or unloadable library raises instead of degrading.
+"""
+import ctypes
+import functools
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libcucm.so")
+
+FORM_AUTO, FORM_PLAIN, FORM_PERSISTENT = 0, 1, 2
+
+CUCM_OK = 0
+_ERRORS = {
+    -1: "EINVAL", -2: "ENOSPC", -3: "EFORMAT", -4: "ENOMEM", -5: "ECUDA",
+    -6: "ENODEV", -7: "ETIMEOUT", -8: "EBUSY", -9: "ENOTFOUND",
+}
+
+
+class CucmError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = lib().cucm_strerror(status).decode()
+        super().__init__("%s: %s (%s)" % (what or "cucm", msg, _ERRORS.get(status, status)))
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("chunksize", ctypes.c_uint64), ("unit", ctypes.c_uint32),
+                ("prelearn", ctypes.c_uint64), ("batch", ctypes.c_uint32)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("form", ctypes.c_int), ("spec_bits", ctypes.c_int),
+                ("max_slots", ctypes.c_int), ("hbm_budget", ctypes.c_uint64)]
+
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+# (name, restype, argtypes) for every entry point of include/cucm.h
+SIGNATURES = [
+    ("cucm_default_params", None, [ctypes.POINTER(Params)]),
+    ("cucm_strerror", ctypes.c_char_p, [ctypes.c_int]),
+    ("cucm_version", ctypes.c_char_p, []),
+    ("cucm_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_void_p)]),
+    ("cucm_ctx_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("cucm_ctx_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    ("cucm_compress_bound", ctypes.c_uint64, [ctypes.c_uint64, ctypes.POINTER(Params)]),
+    ("cucm_decompressed_size", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    ("cucm_compress", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Params),
+                                     ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    ("cucm_decompress", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                       ctypes.c_uint64, _u64p]),
+    ("cucm_compress_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Params),
+                                         ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    ("cucm_decompress_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                           ctypes.c_uint64, _u64p]),
+    ("cucm_compress_batch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                           ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    ("cucm_decompress_batch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                             ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64]),
+    ("cucm_compress_many", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), _u64p,
+                                          ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p), _u64p, _u64p,
+                                          ctypes.POINTER(ctypes.c_int)]),
+    ("cucm_decompress_many", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), _u64p,
+                                            ctypes.POINTER(ctypes.c_void_p), _u64p, _u64p,
+                                            ctypes.POINTER(ctypes.c_int)]),
+    ("cucm_last_device_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("cucm_last_launches", ctypes.c_int, [ctypes.c_void_p, _u64p]),
+]
+
+
+@functools.lru_cache(maxsize=1)
+def lib():
+    """Load libcucm.so (built in-tree by cucm_b200.build)."""
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libcucm.so is not built; run `python -m cucm_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+def default_params(chunksize=None, unit=None, prelearn=None, batch=None):
+    p = Params()
+    lib().cucm_default_params(ctypes.byref(p))
+    if chunksize is not None:
+        p.chunksize = int(chunksize)
+    if unit is not None:
+        p.unit = int(unit)
+    if prelearn is not None:
+        p.prelearn = int(prelearn)
+    if batch is not None:
+        p.batch = int(batch)
+    return p
+
+
+def _buf(data):
+    """(pointer, length, keepalive) for bytes-like or numpy input."""
+    try:
+        import numpy as np
+        if isinstance(data, np.ndarray):
+            a = np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+            return a.ctypes.data, a.size, a
+    except ImportError:  # pragma: no cover
+        pass
+    b = bytes(data)
+    cb = ctypes.create_string_buffer(b, len(b)) if b else ctypes.create_string_buffer(1)
+    return ctypes.addressof(cb), len(b), cb
+
+
+class Context:
+    """One CUDA device, one stream and the device pools of the coder."""
+
+    def __init__(self, device=0, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0):
+        self._h = ctypes.c_void_p()
+        t = Tuning(form, spec_bits, max_slots, hbm_budget)
+        rc = lib().cucm_ctx_create(int(device), ctypes.byref(t), ctypes.byref(self._h))
+        if rc:
+            raise CucmError(rc, "cucm_ctx_create")
+
+    def close(self):
+        if self._h:
+            lib().cucm_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tuning(self, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0):
+        t = Tuning(form, spec_bits, max_slots, hbm_budget)
+        rc = lib().cucm_ctx_set_tuning(self._h, ctypes.byref(t))
+        if rc:
+            raise CucmError(rc, "cucm_ctx_set_tuning")
+
+    def compress(self, data, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+        p = default_params(chunksize, unit, prelearn, batch)
+        ptr, n, keep = _buf(data)
+        cap = lib().cucm_compress_bound(n, ctypes.byref(p))
+        out = ctypes.create_string_buffer(max(cap, 1))
+        got = ctypes.c_uint64()
+        rc = lib().cucm_compress(self._h, ptr, n, ctypes.byref(p), out, cap, ctypes.byref(got))
+        if rc:
+            raise CucmError(rc, "cucm_compress")
+        return out.raw[:got.value]
+
+    def decompress(self, blob):
+        ptr, n, keep = _buf(blob)
+        size = ctypes.c_uint64()
+        rc = lib().cucm_decompressed_size(ptr, n, ctypes.byref(size))
+        if rc:
+            raise CucmError(rc, "cucm_decompressed_size")
+        out = ctypes.create_string_buffer(max(size.value, 1))
+        got = ctypes.c_uint64()
+        rc = lib().cucm_decompress(self._h, ptr, n, out, size.value, ctypes.byref(got))
+        if rc:
+            raise CucmError(rc, "cucm_decompress")
+        return out.raw[:got.value]
+
+    def compress_dev(self, d_in, n, d_out, cap, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+        """Device pointers in and out; returns the container size."""
+        p = default_params(chunksize, unit, prelearn, batch)
+        got = ctypes.c_uint64()
+        rc = lib().cucm_compress_dev(self._h, d_in, n, ctypes.byref(p), d_out, cap, ctypes.byref(got))
+        if rc:
+            raise CucmError(rc, "cucm_compress_dev")
+        return got.value
+
+    def decompress_dev(self, d_in, n, d_out, cap):
+        got = ctypes.c_uint64()
+        rc = lib().cucm_decompress_dev(self._h, d_in, n, d_out, cap, ctypes.byref(got))
+        if rc:
+            raise CucmError(rc, "cucm_decompress_dev")
+        return got.value
+
+    def compress_batch(self, data, chunksize, unitlength=128):
+        ptr, n, keep = _buf(data)
+        nchunks = (n + chunksize - 1) // chunksize
+        cap = nchunks * (4 + 32 * chunksize + 1) + 16
+        out = ctypes.create_string_buffer(max(cap, 1))
+        got = ctypes.c_uint64()
+        rc = lib().cucm_compress_batch(self._h, ptr, n, chunksize, unitlength, out, cap, ctypes.byref(got))
+        if rc:
+            raise CucmError(rc, "cucm_compress_batch")
+        return out.raw[:got.value]
+
+    def decompressbatch(self, body, out_size, chunksize, unitlength=128):
+        ptr, n, keep = _buf(body)
+        out = ctypes.create_string_buffer(max(out_size, 1))
+        rc = lib().cucm_decompress_batch(self._h, ptr, n, chunksize, unitlength, out, out_size)
+        if rc:
+            raise CucmError(rc, "cucm_decompress_batch")
+        return out.raw[:out_size]
+
+    def compress_many(self, buffers, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+        p = default_params(chunksize, unit, prelearn, batch)
+        k = len(buffers)
+        bufs = [_buf(b) for b in buffers]
+        ins = (ctypes.c_void_p * k)(*[b[0] for b in bufs])
+        ns = (ctypes.c_uint64 * k)(*[b[1] for b in bufs])
+        caps = [lib().cucm_compress_bound(b[1], ctypes.byref(p)) for b in bufs]
+        outs_b = [ctypes.create_string_buffer(max(c, 1)) for c in caps]
+        outs = (ctypes.c_void_p * k)(*[ctypes.addressof(o) for o in outs_b])
+        capa = (ctypes.c_uint64 * k)(*caps)
+        got = (ctypes.c_uint64 * k)()
+        st = (ctypes.c_int * k)()
+        rc = lib().cucm_compress_many(self._h, k, ins, ns, ctypes.byref(p), outs, capa, got, st)
+        if rc:
+            raise CucmError(rc, "cucm_compress_many")
+        return [outs_b[i].raw[:got[i]] for i in range(k)]
+
+    def decompress_many(self, blobs):
+        k = len(blobs)
+        bufs = [_buf(b) for b in blobs]
+        sizes = []
+        for p_, n_, _ in bufs:
+            s = ctypes.c_uint64()
+            rc = lib().cucm_decompressed_size(p_, n_, ctypes.byref(s))
+            if rc:
+                raise CucmError(rc, "cucm_decompressed_size")
+            sizes.append(s.value)
+        ins = (ctypes.c_void_p * k)(*[b[0] for b in bufs])
+        ns = (ctypes.c_uint64 * k)(*[b[1] for b in bufs])
+        outs_b = [ctypes.create_string_buffer(max(s, 1)) for s in sizes]
+        outs = (ctypes.c_void_p * k)(*[ctypes.addressof(o) for o in outs_b])
+        capa = (ctypes.c_uint64 * k)(*sizes)
+        got = (ctypes.c_uint64 * k)()
+        st = (ctypes.c_int * k)()
+        rc = lib().cucm_decompress_many(self._h, k, ins, ns, outs, capa, got, st)
+        if rc:
+            raise CucmError(rc, "cucm_decompress_many")
+        return [outs_b[i].raw[:got[i]] for i in range(k)]
+
+    def last_device_ms(self):
+        v = ctypes.c_double()
+        lib().cucm_last_device_ms(self._h, ctypes.byref(v))
+        return v.value
+
+    def last_launches(self):
+        v = ctypes.c_uint64()
+        lib().cucm_last_launches(self._h, ctypes.byref(v))
+        return v.value
+
+
+_default_ctx = None
+
+
+def _ctx():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def compress(data, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+    """Whole container, byte-identical to the reference CLI's output."""
+    return _ctx().compress(data, chunksize, unit, prelearn, batch)
+
+
+def decompress(blob):
+    return _ctx().decompress(blob)
+
+
+def compress_batch(data, chunksize, unitlength=128):
+    """Batch body (big-endian chunk end offsets + payloads) of `data`, coded
+    from the zero model, as compress_batch() returns it."""
+    return _ctx().compress_batch(data, chunksize, unitlength)
+
+
+def decompressbatch(body, out_size, chunksize, unitlength=128):
+    return _ctx().decompressbatch(body, out_size, chunksize, unitlength)
+
+
+def compress_file(in_path, out_path, chunksize=1 << 20, unitlength=128, prelearn_size=0, batch_num=100,
+                  chunknum=-1):
+    with open(in_path, "rb") as f:
+        data = f.read()
+    if chunknum > 0:
+        data = data[:chunksize * chunknum]
+    blob = compress(data, chunksize, unitlength, prelearn_size, batch_num)
+    with open(out_path, "wb") as f:
+        f.write(blob)
+    return len(blob)
+
+
+def decompress_file(in_path, out_path):
+    with open(in_path, "rb") as f:
+        blob = f.read()
+    data = decompress(blob)
+    with open(out_path, "wb") as f:
+        f.write(data)
+    return len(data)

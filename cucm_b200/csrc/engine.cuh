@@ -1,0 +1,59 @@
+// engine.cuh -- device-side job descriptors and host-side engine interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "model.cuh"
+
+namespace cucm {
+
+// Per-chunk model initial state (statep + mixer weights); the slot tables
+// hold the bit-history states.
+struct ModelInit {
+  uint32_t statep[kOrders][256];
+  int32_t w[kMixCtx * kOrders];
+};
+
+// One chunk of work.  All pointers are device pointers.
+struct ChunkTask {
+  const uint8_t *in;     // compress: chunk input; decompress: chunk payload
+  uint8_t *out;          // compress: payload scratch; decompress: output bytes
+  uint64_t in_len;       // compress: input bytes; decompress: payload bytes
+  uint64_t out_cap;      // compress: scratch capacity; decompress: output bytes (len)
+  uint32_t cs;           // chunk size of the stream (format field)
+  uint32_t unit;         // unit length in bits (format field)
+  uint64_t *result;      // compress: payload length written here (or > cap on overflow)
+};
+
+// Status words written by the kernels (per launch).
+enum DevStatus : uint32_t {
+  kDevOk = 0,
+  kDevOverflow = 1,      // some chunk's payload exceeded its scratch capacity
+  kDevBadTask = 2,       // malformed task (unit/size out of range)
+};
+
+struct EngineConfig {
+  int threads = 256;           // CTA size (multiple of 64)
+  int spec_bits = 4;           // decoder speculation depth (1..8); never changes output
+};
+
+cudaError_t upload_tables();  // once per device (current device)
+
+// Launch helpers (all asynchronous on `stream`).
+// slots: nslots chunk-slot tables of kSlotTableBytes each, already holding
+// the initial model states.  init_tables: a clean copy to restore slots from
+// between chunks (nullptr = restore to zero).  queue: one u32 counter.
+cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
+                            const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
+                            uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit);
+cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
+                              const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
+                              uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit);
+
+size_t compress_smem_bytes(int unit);
+size_t decompress_smem_bytes(int unit, int spec_bits);
+
+}  // namespace cucm

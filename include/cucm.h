@@ -1,0 +1,131 @@
+/*
+ * cucm.h -- C ABI of the B200 CuCM coder (libcucm.so).
+ *
+ * The reference (OceanCT/CuCM) has no library interface: its hot path is two
+ * standalone CUDA programs whose internal entry points are
+ *   compress_batch()   cucm_compress_v2.cu:990-992
+ *   decompressbatch()  cucm_decompress_v2.cu:898-903
+ *   compress_file()    cucm_compress_v2.cu:1151-1154
+ *   decompress()       cucm_decompress_v2.cu:1185
+ * and whose boundary is the CLI plus the container format.  The functions
+ * below are what a binding of that path would call.  Every stream produced
+ * here is byte-identical to the reference's for the same input, chunk size,
+ * unit length, prelearn size and batch count; every stream the reference
+ * writes decodes here.
+ *
+ * Conventions: plain pointers and sizes, int status (0 = ok, < 0 = error,
+ * see cucm_strerror), caller-owned output buffers sized with the *_bound /
+ * cucm_decompressed_size queries.  A context owns one CUDA device, one
+ * stream and its device memory pools; calls on one context are serialised
+ * internally, distinct contexts may be used from distinct threads.  There is
+ * no CPU fallback: without a usable B200 (sm_100) every compute call returns
+ * CUCM_ENODEV.
+ */
+#ifndef CUCM_H
+#define CUCM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUCM_OK 0
+#define CUCM_EINVAL (-1)     /* bad argument (size, unit, chunk size, batch) */
+#define CUCM_ENOSPC (-2)     /* output buffer too small */
+#define CUCM_EFORMAT (-3)    /* malformed or truncated container */
+#define CUCM_ENOMEM (-4)     /* device or host allocation failed / over budget */
+#define CUCM_ECUDA (-5)      /* CUDA runtime error */
+#define CUCM_ENODEV (-6)     /* no usable sm_100 device */
+#define CUCM_ETIMEOUT (-7)   /* a bounded device wait expired */
+#define CUCM_EBUSY (-8)      /* serving queue full */
+#define CUCM_ENOTFOUND (-9)  /* unknown request id */
+
+/* Stream parameters: the reference's CLI flags -s -u -p -b
+ * (cucm_compress_v2.cu:1288-1299).  They are stored in the container header
+ * (cucm_compress_v2.cu:1197-1216) and change the bitstream. */
+typedef struct cucm_params {
+  uint64_t chunksize; /* -s, bytes per chunk (default 1 MiB); stored as u32 */
+  uint32_t unit;      /* -u, bits per unit (default 128); multiple of 32, <= 1024 */
+  uint64_t prelearn;  /* -p, bytes of host prelearn prefix (default 0) */
+  uint32_t batch;     /* -b, chunks per container batch (default 100); stored as u16 */
+} cucm_params;
+
+/* Execution choices.  None of them changes a single output byte. */
+typedef enum cucm_form {
+  CUCM_FORM_AUTO = 0,      /* persistent unless told otherwise */
+  CUCM_FORM_PLAIN = 1,     /* one kernel launch per chunk */
+  CUCM_FORM_PERSISTENT = 2 /* one persistent launch, device work queue, longest first */
+} cucm_form;
+
+typedef struct cucm_tuning {
+  int form;            /* cucm_form */
+  int spec_bits;       /* decoder speculation depth 1..8 (0 = autotuned) */
+  int max_slots;       /* cap on resident chunk slots (0 = derive from budget) */
+  uint64_t hbm_budget; /* device bytes this context may hold (0 = 90% of free) */
+} cucm_tuning;
+
+typedef struct cucm_ctx cucm_ctx;
+
+void cucm_default_params(cucm_params *p);
+const char *cucm_strerror(int status);
+const char *cucm_version(void);
+
+/* Create a context on CUDA device `device`; `tuning` may be NULL. */
+int cucm_ctx_create(int device, const cucm_tuning *tuning, cucm_ctx **out);
+int cucm_ctx_destroy(cucm_ctx *ctx);
+int cucm_ctx_set_tuning(cucm_ctx *ctx, const cucm_tuning *tuning);
+
+/* Largest container cucm_compress can produce for n input bytes. */
+uint64_t cucm_compress_bound(uint64_t n, const cucm_params *p);
+/* Original size recorded in a container header (first 4 bytes, big endian,
+ * cucm_decompress_v2.cu:1298-1301). */
+int cucm_decompressed_size(const uint8_t *in, uint64_t n, uint64_t *size);
+
+/* Whole container: the output of `cucm_compress -f IN -s -u -p -b`
+ * (compress_file, cucm_compress_v2.cu:1151-1250) / of `cucm_decompress`
+ * (decompress, cucm_decompress_v2.cu:1185-1248).  Host buffers. */
+int cucm_compress(cucm_ctx *ctx, const uint8_t *in, uint64_t n, const cucm_params *p, uint8_t *out,
+                  uint64_t cap, uint64_t *out_n);
+int cucm_decompress(cucm_ctx *ctx, const uint8_t *in, uint64_t n, uint8_t *out, uint64_t cap,
+                    uint64_t *out_n);
+
+/* Same, with device-resident buffers (no host copies of the data). */
+int cucm_compress_dev(cucm_ctx *ctx, const uint8_t *d_in, uint64_t n, const cucm_params *p, uint8_t *d_out,
+                      uint64_t cap, uint64_t *out_n);
+int cucm_decompress_dev(cucm_ctx *ctx, const uint8_t *d_in, uint64_t n, uint8_t *d_out, uint64_t cap,
+                        uint64_t *out_n);
+
+/* One batch body, no container header: `n` bytes of input split into
+ * chunks of `chunksize`, coded from the zero model (compress_batch,
+ * cucm_compress_v2.cu:990-1149 with sm_init = mixer_init = NULL).  Output is
+ * the batch body the reference writes after its u32 size field: C big-endian
+ * u32 chunk end offsets followed by the chunk payloads. */
+int cucm_compress_batch(cucm_ctx *ctx, const uint8_t *in, uint64_t n, uint64_t chunksize, uint32_t unit,
+                        uint8_t *out, uint64_t cap, uint64_t *out_n);
+/* Inverse of cucm_compress_batch (decompressbatch,
+ * cucm_decompress_v2.cu:898-1054): `body` is the batch body, `out_n` the
+ * number of original bytes. */
+int cucm_decompress_batch(cucm_ctx *ctx, const uint8_t *body, uint64_t body_n, uint64_t chunksize, uint32_t unit,
+                          uint8_t *out, uint64_t out_n);
+
+/* Many independent containers in one call (one persistent launch over all
+ * their chunks).  Entry i reads ins[i][0..ns[i]) and writes outs[i] (caps[i]
+ * bytes), its size to out_ns[i] and its status to status[i]. */
+int cucm_compress_many(cucm_ctx *ctx, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                       const cucm_params *p, uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns,
+                       int *status);
+int cucm_decompress_many(cucm_ctx *ctx, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                         uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns, int *status);
+
+/* Device timing of the last call on this context, milliseconds (CUDA
+ * events around the device work only). */
+int cucm_last_device_ms(cucm_ctx *ctx, double *ms);
+/* Number of kernels this context launched in the last call. */
+int cucm_last_launches(cucm_ctx *ctx, uint64_t *n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUCM_H */

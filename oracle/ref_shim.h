@@ -67,9 +67,13 @@ static inline cudaError_t cudaGetLastError() { return cudaSuccess; }
 static inline cudaError_t cudaDeviceSynchronize() { return cudaSuccess; }
 static inline cudaError_t cudaDeviceReset() { return cudaSuccess; }
 
+/* Zero-filled, like the fresh device memory the reference sees on its first
+ * allocations: its decoder reads never-written entries of d_realsmhashes
+ * (cucm_decompress_v2.cu:876) when a chunk's only unit is partial, and a
+ * garbage hash would index far outside the StateMap. */
 template <typename T>
 static inline cudaError_t cudaMalloc(T **p, size_t n) {
-  *p = (T *)malloc(n ? n : 1);
+  *p = (T *)calloc(n ? n : 1, 1);
   return *p ? cudaSuccess : 2;
 }
 static inline cudaError_t cudaFree(void *p) {

@@ -1,0 +1,66 @@
+"""Host-side checks of the C ABI that need no GPU: the library loads,
+exports every entry point that include/cucm.h declares, validates arguments
+and parses container headers."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import cucm_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    with open(os.path.join(ROOT, "include", "cucm.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(cucm_\w+)\s*\(", text)))
+
+
+def test_header_and_binding_agree(cucm_lib):
+    declared = _declared()
+    bound = sorted(n for n, _, _ in cucm_b200.SIGNATURES)
+    assert declared == bound
+
+
+def test_library_exports_all_symbols(cucm_lib):
+    for name in _declared():
+        assert hasattr(cucm_lib, name), name
+
+
+def _no_gpu():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except Exception:
+        return True
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_ctx_create_without_gpu_fails_loudly(cucm_lib):
+    h = ctypes.c_void_p()
+    assert cucm_lib.cucm_ctx_create(0, None, ctypes.byref(h)) == -6  # CUCM_ENODEV
+    with pytest.raises(cucm_b200.CucmError):
+        cucm_b200.Context(0)
+
+
+def test_default_params_match_reference_cli(cucm_lib):
+    p = cucm_b200.default_params()
+    assert (p.chunksize, p.unit, p.prelearn, p.batch) == (1 << 20, 128, 0, 100)
+
+
+def test_compress_bound_and_size_query(cucm_lib):
+    p = cucm_b200.default_params(chunksize=4096)
+    assert cucm_lib.cucm_compress_bound(0, ctypes.byref(p)) == 21 + 8
+    assert cucm_lib.cucm_compress_bound(10000, ctypes.byref(p)) >= 3 * (32 * 4096 + 5)
+    hdr = bytes([0, 1, 0, 0]) + bytes(17)
+    size = ctypes.c_uint64()
+    assert cucm_lib.cucm_decompressed_size(hdr, len(hdr), ctypes.byref(size)) == 0
+    assert size.value == 65536
+    assert cucm_lib.cucm_decompressed_size(hdr, 3, ctypes.byref(size)) == -3
+
+
+def test_strerror(cucm_lib):
+    for s in range(0, -10, -1):
+        assert cucm_lib.cucm_strerror(s)
