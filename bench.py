@@ -1,0 +1,383 @@
+#!/usr/bin/env python3
+"""Benchmark of the CuCM coder on the 256 MiB mixed workload at 1 MiB chunks.
+
+Workload (one "step"): compress the 256 MiB mixed buffer (50% Markov text,
+25% int32 walk, 15% random, 10% runs in 64 KiB blocks; 1 MiB chunks,
+unit 128, no prelearn, batch 100 -- 256 chunks) and decompress the result
+back, byte-exact.  `value` is the round trip in MB/s of uncompressed bytes
+(input bytes / (compress time + decompress time)), whole job over all ranks,
+with the buffers resident in HBM; compress and decompress are also reported
+alone.  The input (256 MiB, plus 48 GiB of chunk tables touched at random)
+is larger than L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own implementation of the path on the
+host cores: its two programs built for the CPU from its unmodified sources
+(oracle/_ref), one chunk per process on all cores, on a bounded sample of
+the same workload.  Under torchrun, rank 0 alone runs it.
+
+Multi-GPU: one process per GPU; each rank codes its own copy of the
+workload (chunks are independent, there is no data-path exchange), so the
+scaling is weak; the timed region is bracketed by barriers and the slowest
+rank's device time is used.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALGO_BYTES_PER_BYTE = 4096  # 8 bits x 8 orders x (32 B sector gather + 32 B write-back)
+PARAMS = dict(chunksize=1 << 20, unit=128, prelearn=0, batch=100)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="persistent", choices=["persistent", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per compress launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "compress_kernel_mixed256M.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+             "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU runs of the reference's own code (oracle/_ref) on a bounded sample.
+
+def _ref_bins():
+    c = os.path.join(ROOT, "oracle", "_ref", "cucm_compress_ref")
+    d = os.path.join(ROOT, "oracle", "_ref", "cucm_decompress_ref")
+    if os.path.exists(c) and os.path.exists(d):
+        return c, d, "reference"
+    cli = os.path.join(ROOT, "oracle", "oracle_cli")
+    if not os.path.exists(cli):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle_cli"], check=True)
+    return cli, cli, "port"
+
+
+def _host_procs():
+    n = os.cpu_count() or 1
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable"):
+                    gb = int(ln.split()[1]) / (1 << 20)
+                    n = min(n, max(1, int(gb / 1.2)))
+    except Exception:
+        pass
+    return max(1, min(n, 64))
+
+
+def cpu_round_trip(data, nchunks, tmp):
+    """Compress then decompress `nchunks` 1 MiB chunks of `data`, one process
+    per chunk, all at once.  Returns (compress_s, decompress_s, kind)."""
+    comp, decomp, kind = _ref_bins()
+    cs = PARAMS["chunksize"]
+    files = []
+    for i in range(nchunks):
+        p = os.path.join(tmp, "c%d.bin" % i)
+        with open(p, "wb") as f:
+            f.write(data[i * cs:(i + 1) * cs].tobytes())
+        files.append(p)
+
+    def run_all(cmds):
+        t = time.perf_counter()
+        procs = [subprocess.Popen(c, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for c in cmds]
+        rcs = [p.wait() for p in procs]
+        if any(rcs):
+            raise RuntimeError("CPU baseline run failed: %s" % rcs)
+        return time.perf_counter() - t
+
+    if kind == "reference":
+        cc = [[comp, "-f", f, "-o", f + ".cucm", "-s", str(cs), "-u", "128", "-b", "100"] for f in files]
+        dd = [[decomp, "-i", f + ".cucm", "-o", f + ".out"] for f in files]
+    else:
+        cc = [[comp, "c", f, f + ".cucm", str(cs), "128", "0", "100", "1"] for f in files]
+        dd = [[decomp, "d", f + ".cucm", f + ".out", "1"] for f in files]
+    tc = run_all(cc)
+    td = run_all(dd)
+    for f in files:
+        with open(f, "rb") as a, open(f + ".out", "rb") as b:
+            if a.read() != b.read():
+                raise RuntimeError("CPU baseline round trip mismatch")
+    return tc, td, kind
+
+
+def cpu_baseline(data):
+    n = _host_procs()
+    with tempfile.TemporaryDirectory() as tmp:
+        tc, td, kind = cpu_round_trip(data, n, tmp)
+    mb = n * PARAMS["chunksize"] / 1e6
+    return {"value": mb / (tc + td), "unit": "MB/s", "cores": n, "kind": kind,
+            "sample": "%d of the 256 chunks (1 MiB each), one process per chunk, compress then decompress" % n,
+            "compress_MBps": mb / tc, "decompress_MBps": mb / td}
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from cucm_b200 import workloads as W
+    data, _ = W.config1()
+    n = _host_procs()
+    times = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for step in range(args.warmup + args.steps):
+            tc, td, kind = cpu_round_trip(data, n, tmp)
+            if step >= args.warmup:
+                times.append((tc, td))
+    tc = sum(t[0] for t in times)
+    td = sum(t[1] for t in times)
+    mb = n * PARAMS["chunksize"] / 1e6 * len(times)
+    value = mb / (tc + td)
+    line = {
+        "impl": "reference", "metric": "compress+decompress round-trip MB/s", "value": value, "unit": "MB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * (tc + td) / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "mixed 256 MiB, 1 MiB chunks (256), unit 128, batch 100; "
+                               "CPU sample of %d chunks per step" % n, "chunksize": PARAMS["chunksize"],
+                   "unit": 128, "batch": 100, "l2": "inputs larger than L2"},
+        "compress_MBps": mb / tc, "decompress_MBps": mb / td,
+        "cpu_baseline": {"value": value, "unit": "MB/s", "cores": n, "kind": kind,
+                         "sample": "%d chunks of 1 MiB per step, one process per chunk" % n},
+        "e2e": {"value": value, "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import numpy as np
+    import torch
+    import cucm_b200 as cc
+    from cucm_b200 import workloads as W
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    data, _ = W.config1()
+    n = data.size
+    form = cc.FORM_PLAIN if args.form == "plain" else cc.FORM_PERSISTENT
+    ctx = cc.Context(local, form=form)
+    p = cc.default_params(**PARAMS)
+    cap = cc.lib().cucm_compress_bound(n, p)
+    d_in = torch.from_numpy(data).to(dev)
+    d_comp = torch.empty(cap, dtype=torch.uint8, device=dev)
+    d_dec = torch.empty(n, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        m = ctx.compress_dev(d_in.data_ptr(), n, d_comp.data_ptr(), cap, **PARAMS)
+        sc = ctx.last_stats()
+        ctx.decompress_dev(d_comp.data_ptr(), m, d_dec.data_ptr(), n)
+        sd = ctx.last_stats()
+        return m, sc, sd
+
+    for _ in range(max(args.warmup, 0)):
+        comp_n, _, _ = step()
+    if not torch.equal(d_dec, d_in):
+        raise SystemExit("round trip mismatch on the device")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    tc = td = kc = kd = 0.0
+    launches = 0
+    for _ in range(args.steps):
+        comp_n, sc, sd = step()
+        tc += sc["device_ms"]
+        td += sd["device_ms"]
+        kc += sc["kernel_ms"]
+        kd += sd["kernel_ms"]
+        launches += sc["launches"] + sd["launches"]
+    barrier()
+    clocks = sampler.stop()
+    tot = torch.tensor([tc + td, tc, td], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    t_all, t_c, t_d = [float(x) for x in tot.tolist()]
+    K = max(args.steps, 1)
+    total_bytes = world * n * K
+    value = total_bytes / (t_all / 1e3) / 1e6
+
+    # End to end through the host-buffer API: pinned host input, host output.
+    e2e = None
+    if not args.no_e2e:
+        h_in = torch.from_numpy(data).pin_memory()
+        ptr = h_in.data_ptr()
+        import ctypes
+        h_out = torch.empty(cap, dtype=torch.uint8).pin_memory()
+        h_back = torch.empty(n, dtype=torch.uint8).pin_memory()
+        got = ctypes.c_uint64()
+        e_ms = 0.0
+        h2d = d2h = 0
+        for i in range(K + 1):
+            rc = cc.lib().cucm_compress(ctx._h, ptr, n, p, h_out.data_ptr(), cap, ctypes.byref(got))
+            if rc:
+                raise cc.CucmError(rc, "cucm_compress")
+            ms1 = ctx.last_stats()["device_ms"]
+            m = got.value
+            rc = cc.lib().cucm_decompress(ctx._h, h_out.data_ptr(), m, h_back.data_ptr(), n, ctypes.byref(got))
+            if rc:
+                raise cc.CucmError(rc, "cucm_decompress")
+            ms2 = ctx.last_stats()["device_ms"]
+            if i > 0:  # first pass warms the host-buffer path
+                e_ms += ms1 + ms2
+                h2d += n + m
+                d2h += m + n
+        if not torch.equal(h_back, h_in):
+            raise SystemExit("host round trip mismatch")
+        et = torch.tensor([e_ms], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * n * K / (float(et.item()) / 1e3) / 1e6, "unit": "MB/s",
+               "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = measured_peak()
+    kc_launch = kc / K
+    achieved = ALGO_BYTES_PER_BYTE * n / (kc_launch / 1e3) / 1e9 if kc_launch > 0 else None
+    traffic = profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "peak_source": peak_kind, "kernel": "compress_fast_kernel",
+                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_BYTE * n,
+                "kernel_ms_per_launch": kc_launch}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(data)
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "error": str(e)}
+    line = {
+        "metric": "compress+decompress round-trip MB/s", "value": value, "unit": "MB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_all / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "mixed 256 MiB per rank, 1 MiB chunks (256), unit 128, batch 100",
+                   "form": args.form, "chunksize": PARAMS["chunksize"], "unit": 128, "batch": 100,
+                   "parallelism": "independent chunks per rank", "l2": "inputs larger than L2"},
+        "compress_MBps": world * n * K / (t_c / 1e3) / 1e6, "decompress_MBps": world * n * K / (t_d / 1e3) / 1e6,
+        "compressed_bytes": int(comp_n), "ratio": n / comp_n,
+        "kernel_ms": {"compress": kc / K, "decompress": kd / K},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

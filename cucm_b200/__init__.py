@@ -41,9 +41,14 @@ class Params(ctypes.Structure):
                 ("prelearn", ctypes.c_uint64), ("batch", ctypes.c_uint32)]
 
 
+class Stats(ctypes.Structure):
+    _fields_ = [("device_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double),
+                ("launches", ctypes.c_uint64), ("chunks", ctypes.c_uint64)]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("spec_bits", ctypes.c_int),
-                ("max_slots", ctypes.c_int), ("hbm_budget", ctypes.c_uint64)]
+                ("max_slots", ctypes.c_int), ("hbm_budget", ctypes.c_uint64), ("kernel", ctypes.c_int)]
 
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
@@ -79,6 +84,7 @@ SIGNATURES = [
                                             ctypes.POINTER(ctypes.c_int)]),
     ("cucm_last_device_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("cucm_last_launches", ctypes.c_int, [ctypes.c_void_p, _u64p]),
+    ("cucm_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
 ]
 
 
@@ -126,9 +132,9 @@ def _buf(data):
 class Context:
     """One CUDA device, one stream and the device pools of the coder."""
 
-    def __init__(self, device=0, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0):
+    def __init__(self, device=0, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0):
         self._h = ctypes.c_void_p()
-        t = Tuning(form, spec_bits, max_slots, hbm_budget)
+        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel)
         rc = lib().cucm_ctx_create(int(device), ctypes.byref(t), ctypes.byref(self._h))
         if rc:
             raise CucmError(rc, "cucm_ctx_create")
@@ -150,8 +156,8 @@ class Context:
         except Exception:
             pass
 
-    def set_tuning(self, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0):
-        t = Tuning(form, spec_bits, max_slots, hbm_budget)
+    def set_tuning(self, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0):
+        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel)
         rc = lib().cucm_ctx_set_tuning(self._h, ctypes.byref(t))
         if rc:
             raise CucmError(rc, "cucm_ctx_set_tuning")
@@ -263,6 +269,11 @@ class Context:
         v = ctypes.c_uint64()
         lib().cucm_last_launches(self._h, ctypes.byref(v))
         return v.value
+
+    def last_stats(self):
+        st = Stats()
+        lib().cucm_last_stats(self._h, ctypes.byref(st))
+        return dict(device_ms=st.device_ms, kernel_ms=st.kernel_ms, launches=st.launches, chunks=st.chunks)
 
 
 _default_ctx = None

@@ -133,8 +133,12 @@ struct cucm_ctx {
   DevBuf d_init;   // ModelInit
   DevBuf d_tasks, d_results, d_queue, d_status, d_scratch, d_pack, d_body, d_out;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around the engine launches
   double last_ms = 0.0;
+  double kernel_ms = 0.0;
+  bool kernel_pending = false;
   uint64_t launches = 0;
+  uint64_t chunks = 0;
   bool timing_open = false;
 };
 
@@ -189,14 +193,14 @@ int ensure_slots(cucm_ctx *c, uint32_t want, uint64_t other_bytes) {
 }
 
 int resident_ctas(cucm_ctx *c, bool decode, int unit, int spec) {
-  // CTAs of the engine that fit on the device at once.
-  int per_sm = 0;
-  size_t smem = decode ? decompress_smem_bytes(unit, spec) : compress_smem_bytes(unit);
-  (void)smem;
-  // 256 threads x <= 96 registers and <= ~56 KB shared: 2..3 per SM.  A
-  // conservative static figure avoids querying the occupancy API for a
-  // kernel symbol that lives in another translation unit.
-  per_sm = smem <= 70 * 1024 ? 3 : (smem <= 110 * 1024 ? 2 : 1);
+  // CTAs of the engine that fit on the device at once: the pipelined
+  // compressor (448 threads, <= 72 registers) runs 2 per SM; the generic
+  // kernels (256 threads) 3 per SM while their shared memory allows.
+  const bool fast = !decode && c->tuning.kernel != 1 && compress_threads(unit) > 256;
+  const size_t smem = decode ? decompress_smem_bytes(unit, spec) : compress_smem_bytes(unit);
+  int per_sm = fast ? 2 : 3;
+  if (smem > 110 * 1024) per_sm = 1;
+  else if (smem > 72 * 1024 && per_sm > 2) per_sm = 2;
   return per_sm * c->sm_count;
 }
 
@@ -223,9 +227,21 @@ int upload_model(cucm_ctx *c, const ModelSource &ms) {
 
 void timing_begin(cucm_ctx *c) {
   c->launches = 0;
+  c->chunks = 0;
+  c->kernel_ms = 0.0;
+  c->kernel_pending = false;
   cudaEventRecord(c->ev0, c->stream);
   c->timing_open = true;
 }
+// Adds the engine time recorded by the last run_engine (the stream must have
+// been synchronised past evk1).
+void collect_kernel_ms(cucm_ctx *c) {
+  if (!c->kernel_pending) return;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, c->evk0, c->evk1) == cudaSuccess) c->kernel_ms += ms;
+  c->kernel_pending = false;
+}
+
 void timing_end(cucm_ctx *c) {
   if (!c->timing_open) return;
   cudaEventRecord(c->ev1, c->stream);
@@ -233,6 +249,7 @@ void timing_end(cucm_ctx *c) {
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
+  collect_kernel_ms(c);
   c->timing_open = false;
 }
 
@@ -245,12 +262,15 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
   if (n == 0) return CUCM_OK;
   EngineConfig cfg;
   cfg.spec_bits = c->tuning.spec_bits > 0 ? c->tuning.spec_bits : 4;
+  cfg.generic = c->tuning.kernel == 1;
   const int form = c->tuning.form == CUCM_FORM_PLAIN ? CUCM_FORM_PLAIN : CUCM_FORM_PERSISTENT;
 
   int rc = upload_model(c, ms);
   if (rc) return rc;
   CK(c->d_status.ensure(sizeof(uint32_t)));
   CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(uint32_t), c->stream));
+  collect_kernel_ms(c);
+  c->chunks += n;
 
   if (form == CUCM_FORM_PERSISTENT) {
     // Longest first: model work grows with the input bytes, coder work with
@@ -272,6 +292,7 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
     CK(c->d_queue.ensure(sizeof(uint32_t)));
     CK(cudaMemsetAsync(c->d_queue.p, 0, sizeof(uint32_t), c->stream));
     const uint8_t *img = ms.image ? c->image.as<uint8_t>() : nullptr;
+    CK(cudaEventRecord(c->evk0, c->stream));
     cudaError_t e = decode ? launch_decompress(c->d_tasks.as<ChunkTask>(), n, c->slots.as<uint8_t>(), grid, img,
                                                c->d_init.as<ModelInit>(), c->d_queue.as<uint32_t>(),
                                                c->d_status.as<uint32_t>(), cfg, c->stream, unit)
@@ -279,6 +300,8 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
                                              c->d_init.as<ModelInit>(), c->d_queue.as<uint32_t>(),
                                              c->d_status.as<uint32_t>(), cfg, c->stream, unit);
     CK(e);
+    CK(cudaEventRecord(c->evk1, c->stream));
+    c->kernel_pending = true;
     c->launches += 1;
   } else {
     // Plain form: one single-CTA launch per chunk.  At most 128 grids can be
@@ -300,6 +323,7 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
     CK(cudaMemsetAsync(c->d_queue.p, 0, sizeof(uint32_t) * n, c->stream));
     cudaEvent_t fork;
     CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CK(cudaEventRecord(c->evk0, c->stream));
     CK(cudaEventRecord(fork, c->stream));
     for (uint32_t s = 0; s < S; s++) CK(cudaStreamWaitEvent(c->side[s], fork, 0));
     const uint8_t *img = ms.image ? c->image.as<uint8_t>() : nullptr;
@@ -327,6 +351,8 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
       cudaEventDestroy(done);
     }
     cudaEventDestroy(fork);
+    CK(cudaEventRecord(c->evk1, c->stream));
+    c->kernel_pending = true;
   }
   return CUCM_OK;
 }
@@ -632,6 +658,8 @@ int cucm_ctx_create(int device, const cucm_tuning *tuning, cucm_ctx **out) {
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&c->ev0));
   CK(cudaEventCreate(&c->ev1));
+  CK(cudaEventCreate(&c->evk0));
+  CK(cudaEventCreate(&c->evk1));
   CK(upload_tables());
   CK(cudaDeviceSynchronize());
   *out = c.release();
@@ -649,6 +677,8 @@ int cucm_ctx_destroy(cucm_ctx *c) {
   cudaStreamDestroy(c->stream);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
+  cudaEventDestroy(c->evk0);
+  cudaEventDestroy(c->evk1);
   delete c;
   return CUCM_OK;
 }
@@ -936,6 +966,15 @@ int cucm_last_device_ms(cucm_ctx *c, double *ms) {
 int cucm_last_launches(cucm_ctx *c, uint64_t *n) {
   if (!c || !n) return CUCM_EINVAL;
   *n = c->launches;
+  return CUCM_OK;
+}
+
+int cucm_last_stats(cucm_ctx *c, cucm_stats *st) {
+  if (!c || !st) return CUCM_EINVAL;
+  st->device_ms = c->last_ms;
+  st->kernel_ms = c->kernel_ms;
+  st->launches = c->launches;
+  st->chunks = c->chunks;
   return CUCM_OK;
 }
 

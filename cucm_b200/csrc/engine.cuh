@@ -38,6 +38,7 @@ enum DevStatus : uint32_t {
 struct EngineConfig {
   int threads = 256;           // CTA size (multiple of 64)
   int spec_bits = 4;           // decoder speculation depth (1..8); never changes output
+  bool generic = false;        // force the generic (non-pipelined) kernels
 };
 
 cudaError_t upload_tables();  // once per device (current device)
@@ -54,6 +55,7 @@ cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t
                               uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit);
 
 size_t compress_smem_bytes(int unit);
+int compress_threads(int unit);
 size_t decompress_smem_bytes(int unit, int spec_bits);
 
 }  // namespace cucm

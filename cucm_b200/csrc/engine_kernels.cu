@@ -224,26 +224,30 @@ __device__ inline void write_back(const Smem &s, const Layout &L, uint8_t *slot)
   }
 }
 
-// Coder state of the compress CTA (held by warp 1).
+// Coder state of a compress CTA (held by one warp; lane 0 codes).
 struct Coder {
   uint32_t x1, x2;
   uint64_t head;     // bytes produced
   uint64_t flushed;  // bytes written to global
 };
 
-// Lane 0 codes prm[0..n); the ring never overruns because at most 4 bytes
-// per bit are produced and at least stage - 4U bytes are free.
-__device__ inline void coder_run(Coder &c, const Smem &s, const Layout &L, int n) {
+// Lane 0 codes prm[0..n) (pr << 1 | y entries) into the shared-memory ring;
+// the ring never overruns because at most 4 bytes per bit are produced and
+// at least stage - 4U bytes are free.  The split point is
+// x1 + floor((x2 - x1) * pr / 4096), which equals the reference's
+// (r >> 12) * pr + ((r & 0xfff) * pr >> 12) (cucm_compress_v2.cu:855-856)
+// because (r >> 12) * pr is exact.
+__device__ inline void coder_run_p(Coder &c, const uint16_t *prm, uint8_t *stage, int stage_size, int n) {
   if ((threadIdx.x & 31) == 0) {
     uint32_t x1 = c.x1, x2 = c.x2;
     uint64_t head = c.head;
-    const uint32_t mask = (uint32_t)L.stage - 1;
+    const uint32_t mask = (uint32_t)stage_size - 1;
     for (int j = 0; j < n; j++) {
-      uint32_t e = s.prm[j];
-      uint32_t xmid = coder_mid(x1, x2, e >> 1);
-      if (e & 1) x2 = xmid; else x1 = xmid + 1;
+      const uint32_t e = prm[j];
+      const uint32_t f = (uint32_t)(((uint64_t)(x2 - x1) * (e >> 1)) >> 12);
+      if (e & 1) x2 = x1 + f; else x1 = x1 + f + 1;
       while (((x1 ^ x2) & 0xff000000u) == 0) {
-        s.stage[(uint32_t)head & mask] = (uint8_t)(x2 >> 24);
+        stage[(uint32_t)head & mask] = (uint8_t)(x2 >> 24);
         head++;
         x1 <<= 8;
         x2 = (x2 << 8) | 255u;
@@ -260,13 +264,13 @@ __device__ inline void coder_run(Coder &c, const Smem &s, const Layout &L, int n
 }
 
 // Warp-wide copy of complete 512-byte blocks from the ring to global.
-__device__ inline void coder_flush_blocks(Coder &c, const Smem &s, const Layout &L, uint8_t *out, uint64_t cap) {
+__device__ inline void coder_flush_p(Coder &c, const uint8_t *stage, int stage_size, uint8_t *out, uint64_t cap) {
   const int lane = threadIdx.x & 31;
-  const uint32_t mask = (uint32_t)L.stage - 1;
+  const uint32_t mask = (uint32_t)stage_size - 1;
   while (c.head - c.flushed >= kFlushBlock) {
     if (c.flushed + kFlushBlock <= cap) {
-      uint32_t src = ((uint32_t)c.flushed & mask) + lane * 16;
-      uint4 v = *reinterpret_cast<const uint4 *>(s.stage + src);
+      const uint32_t src = ((uint32_t)c.flushed & mask) + lane * 16;
+      const uint4 v = *reinterpret_cast<const uint4 *>(stage + src);
       *reinterpret_cast<uint4 *>(out + c.flushed + lane * 16) = v;
     }
     c.flushed += kFlushBlock;
@@ -274,20 +278,29 @@ __device__ inline void coder_flush_blocks(Coder &c, const Smem &s, const Layout 
   __syncwarp();
 }
 
-__device__ inline void coder_finish(Coder &c, const Smem &s, const Layout &L, uint8_t *out, uint64_t cap,
-                                    uint64_t *result) {
+__device__ inline void coder_finish_p(Coder &c, uint8_t *stage, int stage_size, uint8_t *out, uint64_t cap,
+                                      uint64_t *result) {
   const int lane = threadIdx.x & 31;
-  const uint32_t mask = (uint32_t)L.stage - 1;
-  if (lane == 0) {
-    s.stage[(uint32_t)c.head & mask] = (uint8_t)(c.x1 >> 24);  // flush byte, cucm_compress_v2.cu:902
-  }
+  const uint32_t mask = (uint32_t)stage_size - 1;
+  if (lane == 0) stage[(uint32_t)c.head & mask] = (uint8_t)(c.x1 >> 24);  // flush byte, cucm_compress_v2.cu:902
   __syncwarp();
   c.head += 1;
-  coder_flush_blocks(c, s, L, out, cap);
+  coder_flush_p(c, stage, stage_size, out, cap);
   for (uint64_t i = c.flushed + lane; i < c.head; i += 32)
-    if (i < cap) out[i] = s.stage[(uint32_t)i & mask];
+    if (i < cap) out[i] = stage[(uint32_t)i & mask];
   if (lane == 0) *result = c.head;
   __syncwarp();
+}
+
+__device__ inline void coder_run(Coder &c, const Smem &s, const Layout &L, int n) {
+  coder_run_p(c, s.prm, s.stage, L.stage, n);
+}
+__device__ inline void coder_flush_blocks(Coder &c, const Smem &s, const Layout &L, uint8_t *out, uint64_t cap) {
+  coder_flush_p(c, s.stage, L.stage, out, cap);
+}
+__device__ inline void coder_finish(Coder &c, const Smem &s, const Layout &L, uint8_t *out, uint64_t cap,
+                                    uint64_t *result) {
+  coder_finish_p(c, s.stage, L.stage, out, cap, result);
 }
 
 __device__ void compress_one(const ChunkTask &t, uint8_t *slot, const Smem &s, const Layout &L,
@@ -639,9 +652,14 @@ __global__ void __launch_bounds__(256) decompress_kernel(const ChunkTask *tasks,
   }
 }
 
+#include "compress_fast.cuh"
+
 }  // namespace
 
-size_t compress_smem_bytes(int unit) { return make_layout(unit, 0).total; }
+size_t compress_smem_bytes(int unit) {
+  return unit <= kFastMaxUnit ? make_fast_layout(unit).total : make_layout(unit, 0).total;
+}
+int compress_threads(int unit) { return unit <= kFastMaxUnit ? kFastThreads : 256; }
 size_t decompress_smem_bytes(int unit, int spec_bits) {
   (void)spec_bits;
   return make_layout(unit, 0).total + kNodeBytes;
@@ -660,11 +678,19 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
 cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                             const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
                             uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit) {
-  size_t smem = compress_smem_bytes(unit);
+  if (unit <= kFastMaxUnit && !cfg.generic) {
+    const size_t smem = make_fast_layout(unit).total;
+    cudaError_t e = set_smem((const void *)compress_fast_kernel, smem);
+    if (e != cudaSuccess) return e;
+    compress_fast_kernel<<<nslots, kFastThreads, smem, stream>>>(d_tasks, ntasks, slots, init_tables, d_init,
+                                                                  d_queue, d_status, unit);
+    return cudaGetLastError();
+  }
+  const size_t smem = make_layout(unit, 0).total;
   cudaError_t e = set_smem((const void *)compress_kernel, smem);
   if (e != cudaSuccess) return e;
-  compress_kernel<<<nslots, cfg.threads, smem, stream>>>(d_tasks, ntasks, slots, init_tables, d_init, d_queue,
-                                                         d_status, unit);
+  compress_kernel<<<nslots, 256, smem, stream>>>(d_tasks, ntasks, slots, init_tables, d_init, d_queue, d_status,
+                                                 unit);
   return cudaGetLastError();
 }
 

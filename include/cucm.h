@@ -64,6 +64,7 @@ typedef struct cucm_tuning {
   int spec_bits;       /* decoder speculation depth 1..8 (0 = autotuned) */
   int max_slots;       /* cap on resident chunk slots (0 = derive from budget) */
   uint64_t hbm_budget; /* device bytes this context may hold (0 = 90% of free) */
+  int kernel;          /* 0 = pipelined kernels where the unit allows, 1 = generic kernels */
 } cucm_tuning;
 
 typedef struct cucm_ctx cucm_ctx;
@@ -124,6 +125,17 @@ int cucm_decompress_many(cucm_ctx *ctx, uint32_t count, const uint8_t *const *in
 int cucm_last_device_ms(cucm_ctx *ctx, double *ms);
 /* Number of kernels this context launched in the last call. */
 int cucm_last_launches(cucm_ctx *ctx, uint64_t *n);
+
+/* Figures of the last call: device_ms as above, kernel_ms the time of the
+ * coder kernels alone (CUDA events around their launches), launches, and
+ * the number of chunks coded. */
+typedef struct cucm_stats {
+  double device_ms;
+  double kernel_ms;
+  uint64_t launches;
+  uint64_t chunks;
+} cucm_stats;
+int cucm_last_stats(cucm_ctx *ctx, cucm_stats *st);
 
 #ifdef __cplusplus
 }
