@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
            "-I" + os.path.join(ROOT, "include")]
 CU_SOURCES = ["engine_kernels.cu", "api.cu"]
-HEADERS = ["model.cuh", "engine.cuh", "tables.h", "host_model.h", "cli_common.h"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
 
 
 def nvcc():

@@ -3,88 +3,102 @@
 // Included by engine_kernels.cu (shares its tables and coder helpers).
 //
 // The reference runs five launches per unit and a host round trip between
-// them (cucm_compress_v2.cu:1067-1090).  Here one CTA of 14 warps codes a
-// chunk with every stage of a unit overlapped with the others:
+// them (cucm_compress_v2.cu:1067-1090).  Here one CTA of 7 warps codes a
+// chunk, each warp owning one stage, all stages of consecutive units
+// overlapped ("tick" t):
 //
-//   state warps (2..9, one per order): the bit-history side of the model.
-//     A slot's state only depends on the bits coded in it, never on the
-//     adaptive probabilities, so this pass runs a unit ahead of everything
-//     else: it computes the keys, gathers the unit's slot states, resolves
-//     repeats of a slot inside the unit (warp match + a small shared hash
-//     table), emits for every (bit, order) the state the StateMap update will
-//     see ("live") and the state the prediction sees ("frozen", the unit-start
-//     value), and writes the unit's final states back to the slot tables
-//     before gathering the next unit.
-//   chain warp (0, lane = order): the only serial model chain left, the
-//     StateMap probability updates in bit order (cucm_compress_v2.cu:592-601),
-//     with the adaptation rate carried next to each probability so that a
-//     step is a handful of ALU ops plus one shared-memory load.
-//   mix warps (10..13, thread = bit): stretch, mixer context, dot product,
-//     squash for the unit (cudamixUnit, cucm_compress_v2.cu:755-792) against
-//     a snapshot of the probabilities taken when the previous chain finished,
-//     then the mixer training deltas (cudaupdateMixer, :794-819).
-//   coder warp (1): the binary arithmetic coder, one unit behind the mix.
+//   front warps (3..6, 128 threads)
+//     * keys of unit t+2 for all 8 orders (one FNV pass per bit,
+//       cucm_compress_v2.cu:723-747), the unit's bits and previous bytes;
+//     * slot links of unit t+1: a shared-memory hash table per order maps
+//       each slot of the unit to a bucket; atomicMin on the bucket gives the
+//       first touch in bit order, so every later touch knows it must read the
+//       state its predecessor left; a probe of the previous unit's table
+//       tells whether the slot was touched one unit earlier;
+//     * gathers of unit t+1's slot states from the tables in HBM;
+//     * stretch, mixer context, mixer output and training of unit t-1
+//       (cudamixUnit / cudaupdateMixer, cucm_compress_v2.cu:755-819) against
+//       a snapshot of the probabilities taken when the previous chain ended.
+//   walker warp (2, lane = order): the bit-history side of the StateMap
+//     update for unit t, in bit order: the state each update sees (live), the
+//     state each prediction saw (frozen = unit-start value), the next state,
+//     written through to the slot table.  It only depends on the bits, never
+//     on the probabilities, so it runs a unit ahead of the chain.
+//   chain warp (0, lane = order): the StateMap probability updates of unit
+//     t-1 in bit order (cucm_compress_v2.cu:592-601); the adaptation rate is
+//     carried next to each probability.
+//   coder warp (1): the binary arithmetic coder for unit t-2.
 //
-// Tick t: state pass of unit t, chain and mix of unit t-1, coder of unit
-// t-2.  After the last data unit the coder keeps coding the stale unit
-// buffer up to the chunk end, exactly like cudaencodeUnit's missing input
-// bound (cucm_compress_v2.cu:850-852).
+// After the last data unit the coder keeps coding the stale unit buffer up
+// to the chunk end, as cudaencodeUnit does (cucm_compress_v2.cu:850-852).
 
-constexpr int kFastWarps = 14;
+constexpr int kFastWarps = 7;
 constexpr int kFastThreads = kFastWarps * 32;
 constexpr int kFastMaxUnit = 256;
-constexpr int kWChain = 0, kWCoder = 1, kWState = 2, kWMix = 10;
-constexpr int kMixThreads = 128;
-constexpr int kSnapThreads = 32 + kMixThreads;
+constexpr int kWChain = 0, kWCoder = 1, kWWalk = 2, kWFront = 3;
+constexpr int kFrontThreads = 128;
+constexpr int kSnapThreads = 32 + kFrontThreads;  // chain + front warps
+constexpr int kWinBytes = kFastMaxUnit / 8 + 8;    // input window of a unit (+7 history bytes)
 
 struct FastLayout {
-  int U, NB, logNB, stage;
-  size_t off_tab, off_rec, off_snap, off_w, off_htk, off_htl, off_hts, off_key, off_st, off_fr, off_yb, off_c1,
-      off_prm, off_stage, total;
+  int U, NSLOT, NBK, logNBK, stage;
+  size_t off_tab, off_rec, off_snap, off_w, off_hk, off_ns, off_key, off_lnk, off_bkt, off_fsw, off_st, off_fr,
+      off_yw, off_c1, off_prm, off_win, off_stage, total;
 };
 
 __host__ __device__ inline FastLayout make_fast_layout(int U) {
   FastLayout L;
   L.U = U;
-  L.NB = next_pow2(2 * U);
-  L.logNB = ilog2(L.NB);
+  L.NSLOT = next_pow2(2 * U);   // hash slots per order and unit (load <= 1/2)
+  L.NBK = L.NSLOT / 4;          // 4-slot buckets, one 16-byte load each
+  L.logNBK = ilog2(L.NBK);
   L.stage = next_pow2(4 * U + 1024);
   if (L.stage < kStageMin) L.stage = kStageMin;
+  const size_t NS = (size_t)L.NSLOT;
   size_t o = 0;
-  L.off_tab = o;   o += sizeof(Tables);
-  L.off_rec = o;   o += sizeof(uint64_t) * kOrders * 256;
-  L.off_snap = o;  o += sizeof(uint32_t) * kOrders * 256;
-  L.off_w = o;     o += sizeof(int32_t) * kMixCtx * kOrders;
-  L.off_htk = o;   o += sizeof(uint32_t) * kOrders * L.NB;
-  L.off_htl = o;   o += (size_t)kOrders * L.NB;
-  L.off_hts = o;   o += (size_t)kOrders * L.NB;
-  L.off_key = o;   o += sizeof(uint32_t) * 2 * kOrders * U;
-  L.off_st = o;    o += (size_t)2 * kOrders * U;
-  L.off_fr = o;    o += (size_t)2 * U * kOrders;
-  L.off_yb = o;    o += (size_t)4 * U;
-  L.off_c1 = o;    o += (size_t)4 * (U / 8) + 16;
-  o = (o + 15) & ~(size_t)15;
-  L.off_prm = o;   o += sizeof(uint16_t) * 2 * U;
-  o = (o + 15) & ~(size_t)15;
-  L.off_stage = o; o += (size_t)L.stage;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o = (o + bytes + 15) & ~(size_t)15;
+    return at;
+  };
+  L.off_tab = take(sizeof(Tables));
+  L.off_rec = take(sizeof(uint64_t) * kOrders * 256);
+  L.off_snap = take(sizeof(uint32_t) * kOrders * 256);
+  L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);
+  L.off_hk = take(sizeof(uint32_t) * 2 * kOrders * NS);    // slot keys + 1, [unit parity][order][slot]
+  L.off_ns = take(sizeof(uint16_t) * 2 * kOrders * NS);    // 0x100 | state once written in the unit
+  L.off_key = take(sizeof(uint32_t) * 2 * kOrders * U);    // [unit parity][bit][order]
+  L.off_lnk = take(sizeof(uint16_t) * 2 * kOrders * U);    // slot + 1 in the previous unit's table, or 0
+  L.off_bkt = take(sizeof(uint16_t) * 2 * kOrders * U);    // slot in this unit's table
+  L.off_fsw = take((size_t)2 * kOrders * U);               // gathered slot states
+  L.off_st = take((size_t)2 * kOrders * U);                // live state
+  L.off_fr = take((size_t)2 * U * kOrders);                // frozen state
+  L.off_yw = take(sizeof(uint32_t) * 4 * (U / 32));        // bits, by unit mod 4
+  L.off_c1 = take((size_t)4 * (U / 8));                    // previous byte per byte, by unit mod 4
+  L.off_prm = take(sizeof(uint16_t) * 2 * U);              // coder input, by unit parity
+  L.off_win = take((size_t)kWinBytes);
+  L.off_stage = take((size_t)L.stage);
   L.total = o;
   return L;
 }
 
 struct FastSmem {
   Tables *tab;
-  uint64_t *rec;     // [8][256]  statep | dt[count] << 32
-  uint32_t *snap;    // [8][256]  statep as of the last finished chain
+  uint64_t *rec;     // [256][8]  statep | dt[count] << 32 | dt[count + 1] << 48
+  uint32_t *snap;    // [256][8]  statep as of the last finished chain
   int32_t *w;        // [80*8]
-  uint32_t *htk;     // [8][NB]   0 = empty, else key + 1
-  uint8_t *htl;      // [8][NB]   latest state of the slot
-  uint8_t *hts;      // [8][NB]   state of the slot at the unit start
-  uint32_t *key;     // [2][8][U]
-  uint8_t *st;       // [2][8][U] live state for the chain
-  uint8_t *fr;       // [2][U][8] frozen state for the mix
-  uint8_t *yb;       // [4][U]
-  uint8_t *c1;       // [4][U/8]  previous byte of each byte of the unit
+  uint32_t *hk;      // [2][8][NSLOT]
+  uint16_t *ns;      // [2][8][NSLOT]
+  uint32_t *key;     // [2][U][8]
+  uint16_t *lnk;     // [2][U][8]
+  uint16_t *bkt;     // [2][U][8]
+  uint8_t *fsw;      // [2][U][8]
+  uint8_t *st;       // [2][U][8]
+  uint8_t *fr;       // [2][U][8]
+  uint32_t *yw;      // [4][U/32]
+  uint8_t *c1;       // [4][U/8]
   uint16_t *prm;     // [2][U]
+  uint8_t *win;      // [kWinBytes]
   uint8_t *stage;
 };
 
@@ -94,15 +108,18 @@ __device__ inline FastSmem carve_fast(uint8_t *b, const FastLayout &L) {
   s.rec = reinterpret_cast<uint64_t *>(b + L.off_rec);
   s.snap = reinterpret_cast<uint32_t *>(b + L.off_snap);
   s.w = reinterpret_cast<int32_t *>(b + L.off_w);
-  s.htk = reinterpret_cast<uint32_t *>(b + L.off_htk);
-  s.htl = b + L.off_htl;
-  s.hts = b + L.off_hts;
+  s.hk = reinterpret_cast<uint32_t *>(b + L.off_hk);
+  s.ns = reinterpret_cast<uint16_t *>(b + L.off_ns);
   s.key = reinterpret_cast<uint32_t *>(b + L.off_key);
+  s.lnk = reinterpret_cast<uint16_t *>(b + L.off_lnk);
+  s.bkt = reinterpret_cast<uint16_t *>(b + L.off_bkt);
+  s.fsw = b + L.off_fsw;
   s.st = b + L.off_st;
   s.fr = b + L.off_fr;
-  s.yb = b + L.off_yb;
+  s.yw = reinterpret_cast<uint32_t *>(b + L.off_yw);
   s.c1 = b + L.off_c1;
   s.prm = reinterpret_cast<uint16_t *>(b + L.off_prm);
+  s.win = b + L.off_win;
   s.stage = b + L.off_stage;
   return s;
 }
@@ -111,181 +128,216 @@ __device__ __forceinline__ void named_barrier(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// Input bytes of unit v for the key computation: window index k holds chunk
-// byte v*U/8 - 7 + k (0 outside [0, len)); lane holds k = lane and lane+32.
-__device__ __forceinline__ void load_unit_window(const uint8_t *in, uint64_t len, int U, int v, int lane,
-                                                 uint32_t &w0, uint32_t &w1) {
-  const int64_t b0 = (int64_t)v * (U / 8) - 7;
-  const int64_t i0 = b0 + lane, i1 = b0 + lane + 32;
-  const int nbytes = U / 8 + 7;
-  w0 = (lane < nbytes && i0 >= 0 && (uint64_t)i0 < len) ? (uint32_t)__ldg(in + i0) : 0u;
-  w1 = (lane + 32 < nbytes && i1 >= 0 && (uint64_t)i1 < len) ? (uint32_t)__ldg(in + i1) : 0u;
+// Barrier ids: 0 = whole CTA, 1 = chain + front (snapshot), 2 = front only.
+__device__ __forceinline__ void front_sync() { named_barrier(2, kFrontThreads); }
+
+__device__ __forceinline__ int fast_nvalid(uint64_t data_bits, int U, int v) {
+  const uint64_t b = (uint64_t)v * U;
+  return (v < 0 || b >= data_bits) ? 0 : (int)(data_bits - b < (uint64_t)U ? data_bits - b : (uint64_t)U);
 }
 
-__device__ __forceinline__ uint32_t window_byte(uint32_t w0, uint32_t w1, int k) {
-  uint32_t a = __shfl_sync(0xffffffffu, w0, k & 31);
-  uint32_t b = __shfl_sync(0xffffffffu, w1, k & 31);
-  return k < 32 ? a : b;
+// Input byte k of unit v's window: chunk byte v*U/8 - 7 + k, 0 outside
+// [0, len).  Thread t < U/8 + 7 loads one byte.
+__device__ __forceinline__ uint32_t window_load(const uint8_t *in, uint64_t len, int U, int v, int t) {
+  const int64_t i = (int64_t)v * (U / 8) - 7 + t;
+  return (t < U / 8 + 7 && i >= 0 && (uint64_t)i < len) ? (uint32_t)__ldg(in + i) : 0u;
 }
 
-// State pass, step 1: keys of unit v for order o; gathers of the slot states
-// into registers.  The order-0 warp also stores the unit's bits and the
-// previous byte of each byte (needed by the chain and the mixer context).
-__device__ __forceinline__ void fast_keys_and_gather(const FastSmem &s, const FastLayout &L, const uint8_t *slot,
-                                                     int o, int lane, int v, int nvalid, uint32_t w0, uint32_t w1,
-                                                     uint32_t gath[kFastMaxUnit / 32]) {
+// Front: keys, bits and previous bytes of unit v from the staged window.
+__device__ __forceinline__ void front_keys(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
   const int U = L.U;
-  uint32_t *key = s.key + ((v & 1) * kOrders + o) * U;
-  uint8_t *yb = s.yb + (v & 3) * U;
+  uint32_t *key = s.key + (v & 1) * kOrders * U;
+  uint32_t *yw = s.yw + (v & 3) * (U / 32);
   uint8_t *c1 = s.c1 + (v & 3) * (U / 8);
-  const uint8_t *tab = slot + table_offset(o);
-  CUCM_UNROLL
-  for (int g = 0; g < kFastMaxUnit / 32; g++) {
-    if (g < U / 32) {
-      const int j = g * 32 + lane;
+  for (int j0 = 0; j0 < U; j0 += kFrontThreads) {
+    const int j = j0 + t;
+    uint32_t y = 0;
+    if (j < nvalid) {
       const int q = j >> 3, r = j & 7;
-      const uint32_t cur = window_byte(w0, w1, q + 7);
+      const uint32_t cur = s.win[q + 7];
       const uint32_t h0 = (1u << r) | (cur >> (8 - r));
+      const uint32_t p1 = s.win[q + 6];
+      uint32_t k8[kOrders];
       uint32_t acc = (kFnvBasis ^ h0) * kFnvPrime;
-      uint32_t prev1 = 0;
-      for (int i = 1; i <= 7; i++) {
-        const uint32_t hb = window_byte(w0, w1, q + 7 - i);
-        if (i == 1) prev1 = hb;
-        if (i <= o) acc = (acc ^ hb) * kFnvPrime;
+      k8[0] = h0;
+      k8[1] = (p1 << 8) | h0;
+      acc = (acc ^ p1) * kFnvPrime;
+      CUCM_UNROLL
+      for (int o = 2; o < kOrders; o++) {
+        acc = (acc ^ (uint32_t)s.win[q + 7 - o]) * kFnvPrime;
+        k8[o] = acc & (kSlots - 1);
       }
-      const uint32_t k = o == 0 ? h0 : (o == 1 ? ((prev1 << 8) | h0) : (acc & (kSlots - 1)));
-      if (j < nvalid) {
-        key[j] = k;
-        gath[g] = __ldcg(tab + k);
-      }
-      if (o == 0 && j < nvalid) {
-        yb[j] = (uint8_t)((cur >> (7 - r)) & 1u);
-        if (r == 0) c1[q] = (uint8_t)prev1;
-      }
+      uint4 *dst = reinterpret_cast<uint4 *>(key + j * kOrders);
+      dst[0] = make_uint4(k8[0], k8[1], k8[2], k8[3]);
+      dst[1] = make_uint4(k8[4], k8[5], k8[6], k8[7]);
+      y = (cur >> (7 - r)) & 1u;
+      if (r == 0) c1[q] = (uint8_t)p1;
     }
+    // 32 consecutive bits per warp instruction: pack them.
+    const uint32_t word = __ballot_sync(0xffffffffu, y != 0);
+    if ((t & 31) == 0 && j < U) yw[j >> 5] = word;
   }
 }
 
-// State pass, step 2: resolve unit v of order o.  Groups of 32 bits in bit
-// order; bits that share a slot inside a group are found with a warp match,
-// across groups through a per-unit hash table (slot -> latest state, state
-// at unit start).  The first touch of a slot in the unit starts from the
-// gathered state.
-__device__ __forceinline__ void fast_resolve(const FastSmem &s, const FastLayout &L, uint8_t *slot, int o, int lane,
-                                             int v, int nvalid, const uint32_t gath[kFastMaxUnit / 32]) {
-  const int U = L.U, NB = L.NB;
-  uint32_t *htk = s.htk + o * NB;
-  uint8_t *htl = s.htl + o * NB;
-  uint8_t *hts = s.hts + o * NB;
-  const uint32_t *key = s.key + ((v & 1) * kOrders + o) * U;
-  const uint8_t *yb = s.yb + (v & 3) * U;
-  uint8_t *st = s.st + ((v & 1) * kOrders + o) * U;
-  uint8_t *fr = s.fr + (v & 1) * U * kOrders;
-  const Tables *t = s.tab;
-  for (int b = lane; b < NB; b += 32) htk[b] = 0;
-  __syncwarp();
-  CUCM_UNROLL
-  for (int g = 0; g < kFastMaxUnit / 32; g++) {
-    if (g < U / 32 && g * 32 < nvalid) {
-      const int j = g * 32 + lane;
-      const bool act = j < nvalid;
-      const uint32_t k = act ? key[j] : (0x80000000u | (uint32_t)lane);
-      const int y = act ? yb[j] : 0;
-      const uint32_t peers = __match_any_sync(0xffffffffu, k);
-      const int leader = __ffs(peers) - 1;
-      const uint32_t lower = peers & ((1u << lane) - 1u);
-      const int rank = __popc(lower);
-      const int cnt = __popc(peers);
-      int ss = 0, ls = 0, pos = 0;
-      if (lane == leader && act) {
-        // Leaders of distinct keys probe side by side, so an empty bucket is
-        // claimed with a compare-and-swap; a lost race moves on.
-        uint32_t b = bucket_of(k, L.logNB);
-        for (;;) {
-          uint32_t kk = htk[b];
-          if (kk == 0) {
-            kk = atomicCAS(&htk[b], 0u, k + 1);
-            if (kk == 0) {
-              ss = ls = (int)(gath[g] & 0xffu);
-              hts[b] = (uint8_t)ss;
-              break;
-            }
-          }
-          if (kk == k + 1) {
-            ss = hts[b];
-            ls = htl[b];
-            break;
-          }
-          b = (b + 1) & (uint32_t)(NB - 1);
-        }
-        pos = (int)b;
-      }
-      ss = __shfl_sync(0xffffffffu, ss, leader);
-      ls = __shfl_sync(0xffffffffu, ls, leader);
-      pos = __shfl_sync(0xffffffffu, pos, leader);
-      // Repeats inside the group: the k-th peer sees the state left by the
-      // (k-1)-th one.
-      const int maxc = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
-      const int pred = rank ? 31 - __clz(lower) : lane;
-      int cur = ls, ns = 0;
-      for (int step = 0; step < maxc; step++) {
-        if (rank == step) ns = t->nex[cur][y];
-        const int vv = __shfl_sync(0xffffffffu, ns, pred);
-        if (rank == step + 1) cur = vv;
-      }
-      if (act) {
-        st[j] = (uint8_t)cur;
-        fr[j * kOrders + o] = (uint8_t)ss;
-        if (rank == cnt - 1) htl[pos] = (uint8_t)ns;
-      }
-      __syncwarp();
+// Slot tables: per order, NSLOT/4 buckets of 4 keys (key + 1, 0 = empty),
+// probed with one 16-byte load per bucket; a full bucket spills to the next.
+__device__ __forceinline__ int slot_insert(uint32_t *row, int logNBK, uint32_t kp) {
+  const uint32_t nbk_mask = (1u << logNBK) - 1u;
+  uint32_t b = bucket_of(kp - 1, logNBK);
+  for (;;) {
+    const uint4 q = *reinterpret_cast<const uint4 *>(row + 4 * b);
+    if (q.x == kp) return 4 * b;
+    if (q.y == kp) return 4 * b + 1;
+    if (q.z == kp) return 4 * b + 2;
+    if (q.w == kp) return 4 * b + 3;
+    const int e = q.x == 0 ? 0 : (q.y == 0 ? 1 : (q.z == 0 ? 2 : (q.w == 0 ? 3 : -1)));
+    if (e < 0) {
+      b = (b + 1) & nbk_mask;
+      continue;
     }
+    const uint32_t old = atomicCAS(row + 4 * b + e, 0u, kp);
+    if (old == 0 || old == kp) return 4 * b + e;
+    // another key took the slot: look at the bucket again
   }
-  // Final states of the unit go to the slot table before the next gather.
+}
+
+__device__ __forceinline__ int slot_find(const uint32_t *row, int logNBK, uint32_t kp) {
+  const uint32_t nbk_mask = (1u << logNBK) - 1u;
+  uint32_t b = bucket_of(kp - 1, logNBK);
+  for (;;) {
+    const uint4 q = *reinterpret_cast<const uint4 *>(row + 4 * b);
+    if (q.x == kp) return 4 * b;
+    if (q.y == kp) return 4 * b + 1;
+    if (q.z == kp) return 4 * b + 2;
+    if (q.w == kp) return 4 * b + 3;
+    if (q.x == 0 || q.y == 0 || q.z == 0 || q.w == 0) return -1;
+    b = (b + 1) & nbk_mask;
+  }
+}
+
+// Front: slots of unit v in its own table, and in the previous unit's.
+__device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
+  const int U = L.U, NS = L.NSLOT;
+  const int n = kOrders * U;
+  uint32_t *hk = s.hk + (v & 1) * kOrders * NS;
+  const uint32_t *hk_prev = s.hk + ((v + 1) & 1) * kOrders * NS;
+  const uint32_t *key = s.key + (v & 1) * kOrders * U;
+  uint16_t *lnk = s.lnk + (v & 1) * kOrders * U;
+  uint16_t *bkt = s.bkt + (v & 1) * kOrders * U;
+  {
+    uint4 *k4 = reinterpret_cast<uint4 *>(hk);
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (int i = t; i < kOrders * NS / 4; i += kFrontThreads) k4[i] = z;
+  }
+  front_sync();
+  for (int e = t; e < n; e += kFrontThreads) {
+    const int j = e >> 3, o = e & 7;
+    if (j >= nvalid) continue;
+    const uint32_t kp = key[e] + 1;
+    bkt[e] = (uint16_t)slot_insert(hk + o * NS, L.logNBK, kp);
+    lnk[e] = (uint16_t)(slot_find(hk_prev + o * NS, L.logNBK, kp) + 1);
+  }
+}
+
+// Walker (lane = order): bit-history updates of unit v in bit order.
+__device__ __forceinline__ void walk_unit(const FastSmem &s, const FastLayout &L, uint8_t *slot, int o, int v,
+                                          int n) {
+  const int U = L.U, NS = L.NSLOT;
+  const uint32_t *hk = s.hk + ((v & 1) * kOrders + o) * NS;  // this unit's slots: key + 1
+  const uint16_t *lnk = s.lnk + (v & 1) * U * kOrders + o;   // interleaved by order: 8 lanes, 8 banks
+  const uint16_t *bkt = s.bkt + (v & 1) * U * kOrders + o;
+  const uint8_t *fsb = s.fsw + (v & 1) * U * kOrders + o;
+  const uint32_t *yw = s.yw + (v & 3) * (U / 32);
+  uint8_t *st = s.st + (v & 1) * U * kOrders + o;
+  uint8_t *fr = s.fr + (v & 1) * U * kOrders + o;
+  uint16_t *ns_cur = s.ns + ((v & 1) * kOrders + o) * NS;
+  const uint16_t *ns_prev = s.ns + (((v + 1) & 1) * kOrders + o) * NS;
   uint8_t *tab = slot + table_offset(o);
-  for (int b = lane; b < NB; b += 32) {
-    const uint32_t kk = htk[b];
-    if (kk) tab[kk - 1] = htl[b];
+  const Tables *tb = s.tab;
+  // Software pipeline: what step j+1 reads and step j does not write is
+  // loaded before step j's stores; the slot's latest state (the one value
+  // step j can change) is forwarded when the slots are equal.
+  auto fetch = [&](int j, int &b, uint32_t &frz, uint32_t &kp, uint32_t &nc) {
+    const uint32_t cross = lnk[j * kOrders];
+    b = bkt[j * kOrders];
+    frz = cross ? (uint32_t)(ns_prev[cross - 1] & 0xffu) : (uint32_t)fsb[j * kOrders];
+    kp = hk[b];
+    nc = ns_cur[b];
+  };
+  int b = 0;
+  uint32_t frz = 0, kp = 0, nc = 0;
+  if (n > 0) fetch(0, b, frz, kp, nc);
+  uint32_t ywd = 0;
+  int prev_b = -1;
+  uint32_t prev_ns = 0;
+  for (int j = 0; j < n; j++) {
+    int b1 = 0;
+    uint32_t frz1 = 0, kp1 = 0, nc1 = 0;
+    if (j + 1 < n) fetch(j + 1, b1, frz1, kp1, nc1);
+    if ((j & 31) == 0) ywd = yw[j >> 5];
+    const uint32_t y = (ywd >> (j & 31)) & 1u;
+    uint32_t live = (nc & 0x100u) ? (nc & 0xffu) : frz;  // earlier touch of the slot in this unit
+    if (b == prev_b) live = prev_ns;
+    const uint32_t ns = tb->nex[live][y];
+    ns_cur[b] = (uint16_t)(0x100u | ns);
+    st[j * kOrders] = (uint8_t)live;
+    fr[j * kOrders] = (uint8_t)frz;
+    tab[kp - 1] = (uint8_t)ns;  // write-through; later touches of the slot overwrite it
+    prev_b = b;
+    prev_ns = ns;
+    b = b1;
+    frz = frz1;
+    kp = kp1;
+    nc = nc1;
   }
-  __syncwarp();
 }
 
-// Chain warp: StateMap probability updates of unit v in bit order, one lane
-// per order.  rec[s] carries dt[count(s)] next to the probability so a step
-// needs one shared load (issued a step early) and a few ALU ops; equal
-// consecutive states forward the fresh value.
+// Chain (lane = order): StateMap probability updates of unit v in bit order.
+// A record is statep | dt[c] << 32 | dt[c+1] << 48 for the state's count c;
+// the count only ever grows by one per update, so a run of updates of one
+// state needs each table value two steps after it is requested, and the
+// record store is deferred by one step so it never waits for that load.
 __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &L, int o, int v, int n) {
   const int U = L.U;
-  const uint8_t *sta = s.st + ((v & 1) * kOrders + o) * U;
-  const uint8_t *yb = s.yb + (v & 3) * U;
-  uint64_t *rec = s.rec + o * 256;
+  const uint8_t *sta = s.st + (v & 1) * U * kOrders + o;
+  const uint32_t *yw = s.yw + (v & 3) * (U / 32);
+  uint64_t *rec = s.rec + o;  // rec[state * 8 + order]
   const uint16_t *dt = s.tab->dt;
   int st = sta[0];
-  int st1 = n > 1 ? sta[1] : 0;
-  uint64_t r = rec[st];
+  int st1 = n > 1 ? sta[kOrders] : 0;
+  const uint64_t r0 = rec[st * kOrders];
+  uint32_t val = (uint32_t)r0, d = (uint32_t)(r0 >> 32) & 0xffffu, dn = (uint32_t)(r0 >> 48);
+  int pst = st;
+  uint64_t pnr = r0;
+  uint32_t ywd = 0;
   for (int j = 0; j < n; j++) {
-    const uint64_t r1 = rec[st1];
-    const int st2 = (j + 2 < n) ? sta[j + 2] : 0;
-    const uint32_t y = yb[j];
-    const uint32_t val = (uint32_t)r, d = (uint32_t)(r >> 32);
+    rec[pst * kOrders] = pnr;  // deferred store of the previous step
+    const uint64_t r1 = rec[st1 * kOrders];
+    const int st2 = (j + 2 < n) ? sta[(j + 2) * kOrders] : 0;
+    if ((j & 31) == 0) ywd = yw[j >> 5];
+    const uint32_t y = (ywd >> (j & 31)) & 1u;
     const uint32_t cnt = val & 1023u;
+    const uint32_t dnn = dt[cnt < 1021u ? cnt + 2 : 1023u];
     const int32_t err = (int32_t)((y << 22) - (val >> 10));
     const uint32_t v2 = val + (((uint32_t)(err >> 3) * d) & 0xfffffc00u) + (cnt < 1023u ? 1u : 0u);
-    const uint32_t d2 = dt[cnt < 1023u ? cnt + 1 : 1023u];
-    const uint64_t nr = (uint64_t)v2 | ((uint64_t)d2 << 32);
-    rec[st] = nr;
-    r = (st1 == st) ? nr : r1;
+    pst = st;
+    pnr = (uint64_t)v2 | ((uint64_t)dn << 32) | ((uint64_t)dnn << 48);
+    const bool fwd = st1 == st;
+    val = fwd ? v2 : (uint32_t)r1;
+    d = fwd ? dn : (uint32_t)(r1 >> 32) & 0xffffu;
+    dn = fwd ? dnn : (uint32_t)(r1 >> 48);
     st = st1;
     st1 = st2;
   }
+  rec[pst * kOrders] = pnr;
 }
 
-// Mix warps: predictions, mixer output and training of unit v; thread t
-// handles bits t and t + 128.
-__device__ __forceinline__ void fast_mix(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
+// Front: predictions, mixer output and training of unit v; thread t handles
+// bits t and t + 128.
+__device__ __forceinline__ void front_mix(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
   const int U = L.U;
   const uint8_t *fr = s.fr + (v & 1) * U * kOrders;
-  const uint8_t *yb = s.yb + (v & 3) * U;
+  const uint32_t *yw = s.yw + (v & 3) * (U / 32);
   const uint8_t *c1 = s.c1 + (v & 3) * (U / 8);
   uint16_t *prm = s.prm + (v & 1) * U;
   const uint16_t *prm_old = s.prm + ((v + 1) & 1) * U;
@@ -295,7 +347,7 @@ __device__ __forceinline__ void fast_mix(const FastSmem &s, const FastLayout &L,
   bool has[2] = {false, false};
   CUCM_UNROLL
   for (int h = 0; h < 2; h++) {
-    const int j = t + h * kMixThreads;
+    const int j = t + h * kFrontThreads;
     if (j < U) {
       if (j < nvalid) {
         const uint64_t f8 = *reinterpret_cast<const uint64_t *>(fr + j * kOrders);
@@ -303,13 +355,13 @@ __device__ __forceinline__ void fast_mix(const FastSmem &s, const FastLayout &L,
         CUCM_UNROLL
         for (int o = 0; o < kOrders; o++) {
           const uint32_t stt = (uint32_t)(f8 >> (8 * o)) & 0xffu;
-          const int sm = tb->stretch[s.snap[o * 256 + stt] >> 20];
+          const int sm = tb->stretch[s.snap[stt * kOrders + o] >> 20];
           smps[h][o] = sm;
           olen += (sm != 1);
         }
         const int cx = olen + (c1[j >> 3] >> 5) * 10;
         const int pr = mix_pr(s.w, cx, smps[h], tb);
-        const int y = yb[j];
+        const int y = (yw[j >> 5] >> (j & 31)) & 1;
         prm[j] = (uint16_t)((pr << 1) | y);
         cxs[h] = cx;
         errs[h] = ((y << 12) - pr) * 7;
@@ -319,7 +371,7 @@ __device__ __forceinline__ void fast_mix(const FastSmem &s, const FastLayout &L,
       }
     }
   }
-  named_barrier(2, kMixThreads);  // every weight read before any update
+  front_sync();  // every weight read before any update
   CUCM_UNROLL
   for (int h = 0; h < 2; h++) {
     if (has[h]) {
@@ -332,6 +384,40 @@ __device__ __forceinline__ void fast_mix(const FastSmem &s, const FastLayout &L,
   }
 }
 
+// Front: table words holding the slot states of unit v, into registers.
+// Each thread takes entries e = t + 128 i (i < 16) of the [8][U] grid.
+constexpr int kGatherRegs = kOrders * kFastMaxUnit / kFrontThreads;  // 16
+
+__device__ __forceinline__ void front_gather(const FastSmem &s, const FastLayout &L, const uint8_t *slot, int t,
+                                             int v, int nvalid, uint32_t g[kGatherRegs]) {
+  const int U = L.U;
+  const uint32_t *key = s.key + (v & 1) * kOrders * U;
+  CUCM_UNROLL
+  for (int i = 0; i < kGatherRegs; i++) {
+    const int e = t + i * kFrontThreads;
+    if (e < kOrders * U) {
+      const int j = e >> 3, o = e & 7;
+      if (j < nvalid) {
+        const uint32_t k = key[e];
+        const uint32_t *p = reinterpret_cast<const uint32_t *>(slot + table_offset(o) + (k & ~3u));
+        g[i] = __ldcg(p);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void front_store_gather(const FastSmem &s, const FastLayout &L, int t, int v,
+                                                   const uint32_t g[kGatherRegs]) {
+  const int U = L.U;
+  const uint32_t *key = s.key + (v & 1) * kOrders * U;
+  uint8_t *fsb = s.fsw + (v & 1) * kOrders * U;
+  CUCM_UNROLL
+  for (int i = 0; i < kGatherRegs; i++) {
+    const int e = t + i * kFrontThreads;
+    if (e < kOrders * U) fsb[e] = (uint8_t)(g[i] >> (8 * (key[e] & 3)));
+  }
+}
+
 __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastSmem &s, const FastLayout &L,
                                   const ModelInit *init, uint32_t *status) {
   const int tid = threadIdx.x;
@@ -341,73 +427,89 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
   const uint64_t total_bits = 8ull * t.cs;
   const uint64_t data_bits = 8ull * len;
   const int nU = (int)((data_bits + U - 1) / U);
-  auto nvalid_of = [&](int v) -> int {
-    const uint64_t b = (uint64_t)v * U;
-    return b >= data_bits ? 0 : (int)(data_bits - b < (uint64_t)U ? data_bits - b : (uint64_t)U);
-  };
+  const bool front = warp >= kWFront;
+  const int ft = tid - kWFront * 32;
   auto ncode_of = [&](int v) -> int {
     const uint64_t b = (uint64_t)v * U;
     return b >= total_bits ? 0 : (int)(total_bits - b < (uint64_t)U ? total_bits - b : (uint64_t)U);
   };
 
   for (int i = tid; i < kOrders * 256; i += blockDim.x) {
-    const uint32_t v = init->statep[i >> 8][i & 255];
-    s.rec[i] = (uint64_t)v | ((uint64_t)s.tab->dt[v & 1023u] << 32);
+    const uint32_t v = init->statep[i & 7][i >> 3];  // rec[state * 8 + order]
+    const uint32_t c = v & 1023u;
+    s.rec[i] = (uint64_t)v | ((uint64_t)s.tab->dt[c] << 32) | ((uint64_t)s.tab->dt[c < 1023u ? c + 1 : 1023u] << 48);
   }
   for (int i = tid; i < kMixCtx * kOrders; i += blockDim.x) s.w[i] = init->w[i];
   for (int i = tid; i < 2 * U; i += blockDim.x) s.prm[i] = 0;  // cucm_compress_v2.cu:1039-1040
+  for (int i = tid; i < 2 * kOrders * L.NSLOT; i += blockDim.x) s.hk[i] = 0;
 
   Coder c{0u, 0xffffffffu, 0, 0};
-  uint32_t gath[kFastMaxUnit / 32];
-  uint32_t w0 = 0, w1 = 0;
-  const bool is_state = warp >= kWState && warp < kWMix;
-  const int so = warp - kWState;
-  if (is_state) {
-    uint32_t a0, a1;
-    load_unit_window(t.in, len, U, 0, lane, a0, a1);
-    __syncthreads();
-    fast_keys_and_gather(s, L, slot, so, lane, 0, nvalid_of(0), a0, a1, gath);
-    if (nU > 1) load_unit_window(t.in, len, U, 1, lane, w0, w1);
-  } else {
-    __syncthreads();
+  uint32_t g[kGatherRegs];
+  uint32_t wbyte = 0;
+  __syncthreads();
+
+  // Prologue: keys of units 0 and 1, links and gathers of unit 0.
+  if (front) {
+    for (int v = 0; v < 2 && v < nU; v++) {
+      const uint32_t b = window_load(t.in, len, U, v, ft);
+      if (ft < U / 8 + 7) s.win[ft] = (uint8_t)b;
+      front_sync();
+      front_keys(s, L, ft, v, fast_nvalid(data_bits, U, v));
+      front_sync();
+    }
+    front_links(s, L, ft, 0, fast_nvalid(data_bits, U, 0));
+    front_gather(s, L, slot, ft, 0, fast_nvalid(data_bits, U, 0), g);
+    front_store_gather(s, L, ft, 0, g);
+    if (nU > 2) wbyte = window_load(t.in, len, U, 2, ft);
   }
   __syncthreads();
 
   for (int tau = 0; tau < nU + 2; tau++) {
     const int um = tau - 1;
-    const bool snap_role = warp == kWChain || warp >= kWMix;
-    if (snap_role) {
+    // gathers of unit tau+1 go out first; they land while the front works
+    const int nv1 = fast_nvalid(data_bits, U, tau + 1);
+    if (front && tau + 1 < nU) front_gather(s, L, slot, ft, tau + 1, nv1, g);
+    if (warp == kWChain || front) {
       if (um >= 0 && um < nU) {
-        const int k = warp == kWChain ? lane : 32 + (tid - kWMix * 32);
+        const int k = warp == kWChain ? lane : 32 + ft;
         for (int i = k; i < kOrders * 256; i += kSnapThreads) s.snap[i] = (uint32_t)s.rec[i];
       }
       named_barrier(1, kSnapThreads);
     }
     if (warp == kWChain) {
-      if (um >= 0 && um < nU && lane < kOrders) fast_chain(s, L, lane, um, nvalid_of(um));
+      if (um >= 0 && um < nU && lane < kOrders) fast_chain(s, L, lane, um, fast_nvalid(data_bits, U, um));
     } else if (warp == kWCoder) {
       const int uc = tau - 2;
       if (uc >= 0 && uc < nU) {
         coder_run_p(c, s.prm + (uc & 1) * U, s.stage, L.stage, ncode_of(uc));
         coder_flush_p(c, s.stage, L.stage, t.out, t.out_cap);
       }
-    } else if (is_state) {
+    } else if (warp == kWWalk) {
       if (tau < nU) {
-        fast_resolve(s, L, slot, so, lane, tau, nvalid_of(tau), gath);
-        if (tau + 1 < nU) {
-          fast_keys_and_gather(s, L, slot, so, lane, tau + 1, nvalid_of(tau + 1), w0, w1, gath);
-          if (tau + 2 < nU) load_unit_window(t.in, len, U, tau + 2, lane, w0, w1);
-        }
+        uint4 *z4 = reinterpret_cast<uint4 *>(s.ns + (tau & 1) * kOrders * L.NSLOT);
+        for (int i = lane; i < kOrders * L.NSLOT / 8; i += 32) z4[i] = make_uint4(0, 0, 0, 0);
+        __syncwarp();
+        if (lane < kOrders) walk_unit(s, L, slot, lane, tau, fast_nvalid(data_bits, U, tau));
       }
     } else {
-      if (um >= 0 && um < nU) fast_mix(s, L, tid - kWMix * 32, um, nvalid_of(um));
+      if (um >= 0 && um < nU) front_mix(s, L, ft, um, fast_nvalid(data_bits, U, um));
+      if (tau + 1 < nU) {
+        front_links(s, L, ft, tau + 1, nv1);
+        if (tau + 2 < nU) {
+          if (ft < U / 8 + 7) s.win[ft] = (uint8_t)wbyte;
+          front_sync();
+          front_keys(s, L, ft, tau + 2, fast_nvalid(data_bits, U, tau + 2));
+          if (tau + 3 < nU) wbyte = window_load(t.in, len, U, tau + 3, ft);
+        }
+        front_store_gather(s, L, ft, tau + 1, g);
+      }
     }
     __syncthreads();
   }
 
   if (warp == kWCoder) {
     const uint16_t *last = s.prm + ((nU - 1) & 1) * U;
-    for (int v = nU; ; v++) {
+    for (int v = nU;; v++) {
       const int n = ncode_of(v);
       if (n <= 0) break;
       coder_run_p(c, last, s.stage, L.stage, n);

@@ -231,36 +231,47 @@ struct Coder {
   uint64_t flushed;  // bytes written to global
 };
 
-// Lane 0 codes prm[0..n) (pr << 1 | y entries) into the shared-memory ring;
-// the ring never overruns because at most 4 bytes per bit are produced and
-// at least stage - 4U bytes are free.  The split point is
-// x1 + floor((x2 - x1) * pr / 4096), which equals the reference's
-// (r >> 12) * pr + ((r & 0xfff) * pr >> 12) (cucm_compress_v2.cu:855-856)
-// because (r >> 12) * pr is exact.
-__device__ inline void coder_run_p(Coder &c, const uint16_t *prm, uint8_t *stage, int stage_size, int n) {
-  if ((threadIdx.x & 31) == 0) {
-    uint32_t x1 = c.x1, x2 = c.x2;
-    uint64_t head = c.head;
-    const uint32_t mask = (uint32_t)stage_size - 1;
-    for (int j = 0; j < n; j++) {
-      const uint32_t e = prm[j];
-      const uint32_t f = (uint32_t)(((uint64_t)(x2 - x1) * (e >> 1)) >> 12);
-      if (e & 1) x2 = x1 + f; else x1 = x1 + f + 1;
-      while (((x1 ^ x2) & 0xff000000u) == 0) {
-        stage[(uint32_t)head & mask] = (uint8_t)(x2 >> 24);
-        head++;
-        x1 <<= 8;
-        x2 = (x2 << 8) | 255u;
-      }
-    }
-    c.x1 = x1;
-    c.x2 = x2;
-    c.head = head;
+// Codes prm[0..n) (pr << 1 | y entries) into the shared-memory ring.  All 32
+// lanes of the calling warp run the same arithmetic on the same data, so the
+// control flow stays warp-uniform; lane 0 alone stores the bytes.  The ring
+// never overruns: at most 4 bytes per bit are produced and at least
+// stage - 4U bytes are free.  The split point x1 + floor((x2 - x1) * pr / 4096)
+// is taken as the high word of (x2 - x1) * (pr << 20); it equals the
+// reference's (r >> 12) * pr + ((r & 0xfff) * pr >> 12)
+// (cucm_compress_v2.cu:855-856) because (r >> 12) * pr is exact.
+__device__ __forceinline__ void coder_step(uint32_t e, uint32_t &x1, uint32_t &x2, uint32_t &head, uint8_t *stage,
+                                           uint32_t mask, bool writer) {
+  const uint32_t xm = x1 + __umulhi(x2 - x1, (e >> 1) << 20);
+  if (e & 1) x2 = xm; else x1 = xm + 1;
+  while ((x1 ^ x2) < 0x1000000u) {
+    if (writer) stage[head & mask] = (uint8_t)(x2 >> 24);
+    head++;
+    x1 <<= 8;
+    x2 = (x2 << 8) | 255u;
   }
+}
+
+__device__ inline void coder_run_p(Coder &c, const uint16_t *prm, uint8_t *stage, int stage_size, int n) {
+  const bool writer = (threadIdx.x & 31) == 0;
+  const uint32_t mask = (uint32_t)stage_size - 1;
+  uint32_t x1 = c.x1, x2 = c.x2;
+  uint32_t head = (uint32_t)c.head;
+  const uint32_t head0 = head;
+  int j = 0;
+  if ((reinterpret_cast<uintptr_t>(prm) & 7) == 0) {
+    for (; j + 4 <= n; j += 4) {
+      const uint64_t e4 = *reinterpret_cast<const uint64_t *>(prm + j);
+      coder_step((uint32_t)e4 & 0xffffu, x1, x2, head, stage, mask, writer);
+      coder_step((uint32_t)(e4 >> 16) & 0xffffu, x1, x2, head, stage, mask, writer);
+      coder_step((uint32_t)(e4 >> 32) & 0xffffu, x1, x2, head, stage, mask, writer);
+      coder_step((uint32_t)(e4 >> 48), x1, x2, head, stage, mask, writer);
+    }
+  }
+  for (; j < n; j++) coder_step(prm[j], x1, x2, head, stage, mask, writer);
+  c.x1 = x1;
+  c.x2 = x2;
+  c.head += (uint32_t)(head - head0);
   __syncwarp();
-  c.x1 = __shfl_sync(0xffffffffu, c.x1, 0);
-  c.x2 = __shfl_sync(0xffffffffu, c.x2, 0);
-  c.head = __shfl_sync(0xffffffffu, (unsigned long long)c.head, 0);
 }
 
 // Warp-wide copy of complete 512-byte blocks from the ring to global.
