@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(kFastThreads, 2)
   const FastLayout L = make_fast_layout(unit);
   const FastSmem s = carve_fast(smem_raw, L);
   uint8_t *slot = slots + (size_t)blockIdx.x * kSlotTableBytes;
-  copy_tables(s.tab);
+  copy_tables(&g_tables, s.tab);
   __shared__ uint32_t s_task;
   bool fresh = true;
   for (;;) {
@@ -553,3 +553,4 @@ __global__ void __launch_bounds__(kFastThreads, 2)
     compress_fast_one(t, slot, s, L, init, status);
   }
 }
+
