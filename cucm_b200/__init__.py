@@ -85,6 +85,9 @@ SIGNATURES = [
     ("cucm_last_device_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("cucm_last_launches", ctypes.c_int, [ctypes.c_void_p, _u64p]),
     ("cucm_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
+    ("cucm_compress_chunk_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                                   ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, _u64p,
+                                                   ctypes.c_void_p]),
 ]
 
 

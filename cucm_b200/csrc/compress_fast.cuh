@@ -554,3 +554,13 @@ __global__ void __launch_bounds__(kFastThreads, 2)
   }
 }
 
+// One chunk, task passed by value, tables at `slot` (no work queue).
+__global__ void __launch_bounds__(kFastThreads, 2)
+    compress_fast_single_kernel(const ChunkTask t, uint8_t *slot, const ModelInit *init, uint32_t *status) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  const FastLayout L = make_fast_layout((int)t.unit);
+  const FastSmem s = carve_fast(smem_raw, L);
+  copy_tables(&g_tables, s.tab);
+  __syncthreads();
+  compress_fast_one(t, slot, s, L, init, status);
+}

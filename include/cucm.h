@@ -137,6 +137,27 @@ typedef struct cucm_stats {
 } cucm_stats;
 int cucm_last_stats(cucm_ctx *ctx, cucm_stats *st);
 
+/* Compress one chunk without allocating any memory.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when
+ * they compress -- code running during a CUDA graph capture, plugins whose
+ * host application owns every device allocation, and paths that cannot pay
+ * for cudaMalloc's synchronisation.
+ * d_in: `len` input bytes in device memory (1 <= len <= chunksize); the
+ * result is that chunk's payload (coded bytes and flush byte) exactly as the
+ * reference codes a chunk of that length in a stream of that chunk size and
+ * unit, stale tail included when len < chunksize.  d_out: device buffer of
+ * `cap` bytes; *out_len receives the payload size (CUCM_ENOSPC if it is
+ * larger than cap).  unit: a multiple of 32 up to 256.  stream: a
+ * cudaStream_t, or NULL for the legacy default stream; the call returns after
+ * the stream has finished it.
+ * The only scratch is a file-scope device array holding one chunk's tables
+ * (192.06 MiB per GPU that calls this, kept until the process exits), so
+ * input longer than one chunk is rejected with CUCM_EINVAL.  All calls share
+ * that array; calls that overlap on the GPU race.  The first call on a device
+ * does the set-up; make it before any stream capture begins. */
+int cucm_compress_chunk_noalloc(const uint8_t *d_in, uint64_t len, uint64_t chunksize, uint32_t unit,
+                                uint8_t *d_out, uint64_t cap, uint64_t *out_len, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
