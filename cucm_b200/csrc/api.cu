@@ -192,16 +192,9 @@ int ensure_slots(cucm_ctx *c, uint32_t want, uint64_t other_bytes) {
   return CUCM_OK;
 }
 
-int resident_ctas(cucm_ctx *c, bool decode, int unit, int spec) {
-  // CTAs of the engine that fit on the device at once: the pipelined
-  // compressor (448 threads, <= 72 registers) runs 2 per SM; the generic
-  // kernels (256 threads) 3 per SM while their shared memory allows.
-  const bool fast = !decode && c->tuning.kernel != 1 && compress_threads(unit) > 256;
-  const size_t smem = decode ? decompress_smem_bytes(unit, spec) : compress_smem_bytes(unit);
-  int per_sm = fast ? 2 : 3;
-  if (smem > 110 * 1024) per_sm = 1;
-  else if (smem > 72 * 1024 && per_sm > 2) per_sm = 2;
-  return per_sm * c->sm_count;
+// Chunks the engine runs at once on the whole device.
+int resident_chunks(cucm_ctx *c, bool decode, int unit, const EngineConfig &cfg) {
+  return engine_slots_per_sm(decode, unit, cfg) * c->sm_count;
 }
 
 int fill_slots(cucm_ctx *c, uint32_t n, const ModelSource &ms) {
@@ -263,6 +256,7 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
   EngineConfig cfg;
   cfg.spec_bits = c->tuning.spec_bits > 0 ? c->tuning.spec_bits : 4;
   cfg.generic = c->tuning.kernel == 1;
+  cfg.sm_count = c->sm_count;
   const int form = c->tuning.form == CUCM_FORM_PLAIN ? CUCM_FORM_PLAIN : CUCM_FORM_PERSISTENT;
 
   int rc = upload_model(c, ms);
@@ -280,7 +274,7 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
       uint64_t lb = (decode ? b.out_cap : b.in_len) * 4 + b.cs;
       return la > lb;
     });
-    uint32_t want = std::min<uint32_t>(n, (uint32_t)resident_ctas(c, decode, unit, cfg.spec_bits));
+    uint32_t want = std::min<uint32_t>(n, (uint32_t)resident_chunks(c, decode, unit, cfg));
     if (c->tuning.max_slots > 0) want = std::min<uint32_t>(want, (uint32_t)c->tuning.max_slots);
     rc = ensure_slots(c, want, other_bytes);
     if (rc) return rc;

@@ -1,0 +1,370 @@
+// decompress_fast.cuh -- chunk decoder, one warp per chunk, units of 32..256 bits.
+//
+// Included by engine_kernels.cu (shares its tables and helpers).
+//
+// The reference decodes a unit in speculation steps of L+1 bits, each step
+// three launches and a host round trip (cucm_decompress_v2.cu:977-1032).
+// Here one warp owns a chunk and decodes it a nibble ("round") at a time:
+//
+//   * the 15 nodes of the nibble's speculation tree (every prefix of 0..3
+//     bits) get their 8 context keys and frozen slot states -- one lane per
+//     node, 8 gathers in flight per lane, so a round costs one memory
+//     round trip;
+//   * while those gathers are in flight the same warp runs the model update
+//     of the previous round's 4 bits (lane = order): the bit-history walk
+//     through a per-unit overlay (slot -> live state), the StateMap
+//     probability chain and the mixer deltas, all in bit order;
+//   * each node lane stretches, mixes and squashes its prediction against
+//     the frozen model, and the warp decodes the 4 bits uniformly (every lane
+//     runs the same coder arithmetic; the split point of a node comes from
+//     its lane by shuffle);
+//   * the 4 lanes on the decoded path record keys, states and inputs of their
+//     bit for the next round's update.
+//
+// At a unit end the overlay's states are written to the slot tables, the
+// live probabilities become the frozen ones and the summed mixer deltas are
+// added to the weights (updateStateMap / updateMixer,
+// cucm_decompress_v2.cu:870-896).  Rounds never straddle a unit or byte
+// boundary: units are multiples of 32 bits.
+//
+// Several warps of a CTA decode independent chunks and share the read-only
+// tables.
+
+constexpr int kDecMaxUnit = 256;
+constexpr int kDecMaxWarps = 8;
+constexpr int kDecWin = 2048;   // payload window per warp (bytes)
+constexpr int kDecNodes = 15;   // nodes of a 4-bit speculation tree
+
+struct DecLayout {
+  int U, NS, logNS, warps;
+  size_t off_spf, off_spl, off_w, off_dw, off_ovk, off_ovs, off_ovl, off_ovn, off_rk, off_rs, off_rsmp, off_rpc,
+      off_win, off_outb, per_warp, off_tab, total;
+};
+
+__host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
+  DecLayout L;
+  L.U = U;
+  L.NS = next_pow2(2 * U);  // overlay slots per order (load <= 1/2)
+  L.logNS = ilog2(L.NS);
+  L.warps = warps;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o = (o + bytes + 15) & ~(size_t)15;
+    return at;
+  };
+  L.off_spf = take(sizeof(uint32_t) * 256 * kOrders);          // frozen statep [state][order]
+  L.off_spl = take(sizeof(uint32_t) * 256 * kOrders);          // live statep [state][order]
+  L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);         // frozen weights
+  L.off_dw = take(sizeof(int32_t) * kMixCtx * kOrders);        // summed deltas of the unit
+  L.off_ovk = take(sizeof(uint32_t) * kOrders * L.NS);         // overlay keys + 1 (0 = empty)
+  L.off_ovs = take((size_t)kOrders * L.NS);                    // overlay live states
+  L.off_ovl = take(sizeof(uint16_t) * U * kOrders);            // overlay entries in use [entry][order]
+  L.off_ovn = take(sizeof(int) * kOrders);
+  L.off_rk = take(sizeof(uint32_t) * 2 * 4 * kOrders);         // records [round parity][bit][order]
+  L.off_rs = take((size_t)2 * 4 * kOrders);
+  L.off_rsmp = take(sizeof(int16_t) * 2 * 4 * kOrders);
+  L.off_rpc = take(sizeof(uint32_t) * 2 * 4);                  // pr | cxt << 16 | y << 24
+  L.off_win = take((size_t)kDecWin);
+  L.off_outb = take((size_t)kDecMaxUnit / 8);
+  L.per_warp = o;
+  L.off_tab = (size_t)warps * L.per_warp;
+  L.total = L.off_tab + ((sizeof(Tables) + 15) & ~(size_t)15);
+  return L;
+}
+
+struct DecSmem {
+  uint32_t *spf, *spl;
+  int32_t *w, *dw;
+  uint32_t *ovk;
+  uint8_t *ovs;
+  uint16_t *ovl;
+  int *ovn;
+  uint32_t *rk;
+  uint8_t *rs;
+  int16_t *rsmp;
+  uint32_t *rpc;
+  uint8_t *win, *outb;
+};
+
+__device__ inline DecSmem carve_dec(uint8_t *base, const DecLayout &L, int warp) {
+  uint8_t *b = base + (size_t)warp * L.per_warp;
+  DecSmem s;
+  s.spf = reinterpret_cast<uint32_t *>(b + L.off_spf);
+  s.spl = reinterpret_cast<uint32_t *>(b + L.off_spl);
+  s.w = reinterpret_cast<int32_t *>(b + L.off_w);
+  s.dw = reinterpret_cast<int32_t *>(b + L.off_dw);
+  s.ovk = reinterpret_cast<uint32_t *>(b + L.off_ovk);
+  s.ovs = b + L.off_ovs;
+  s.ovl = reinterpret_cast<uint16_t *>(b + L.off_ovl);
+  s.ovn = reinterpret_cast<int *>(b + L.off_ovn);
+  s.rk = reinterpret_cast<uint32_t *>(b + L.off_rk);
+  s.rs = b + L.off_rs;
+  s.rsmp = reinterpret_cast<int16_t *>(b + L.off_rsmp);
+  s.rpc = reinterpret_cast<uint32_t *>(b + L.off_rpc);
+  s.win = b + L.off_win;
+  s.outb = b + L.off_outb;
+  return s;
+}
+
+// Warp-wide refill of the payload window so that it starts at or just below
+// payload byte `at`, on a 16-byte boundary of the payload's address (so the
+// window base may lie up to 15 bytes before the payload).  Only 16-byte
+// blocks that hold payload bytes are read.  Returns the payload offset of
+// window byte 0.
+__device__ inline long long dec_refill(uint8_t *win, const uint8_t *pay, uint64_t plen, uint64_t at, int lane) {
+  const uint8_t *a = reinterpret_cast<const uint8_t *>((reinterpret_cast<uintptr_t>(pay) + at) & ~(uintptr_t)15);
+  const uint8_t *end = pay + plen;
+  for (int j = lane; j < kDecWin / 16; j += 32) {
+    const uint8_t *blk = a + 16 * j;
+    if (blk < end) *reinterpret_cast<uint4 *>(win + 16 * j) = *reinterpret_cast<const uint4 *>(blk);
+  }
+  __syncwarp();
+  return (long long)(a - pay);
+}
+
+// Model update of one round's 4 bits for order `o` (one lane per order), in
+// bit order: the live state of each slot (overlay, else the frozen state the
+// prediction saw), its next state, the StateMap probability of the live state
+// (cucm_decompress_v2.cu:870-883) and the mixer deltas (:885-896).
+__device__ __forceinline__ void dec_update_round(const DecSmem &s, const Tables *tab, const DecLayout &L, int o,
+                                                 int buf) {
+  uint32_t *ovk = s.ovk + o * L.NS;
+  uint8_t *ovs = s.ovs + o * L.NS;
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++) {
+    const int r = (buf * 4 + i) * kOrders + o;
+    const uint32_t k = s.rk[r];
+    const uint32_t pc = s.rpc[buf * 4 + i];
+    const int y = (int)(pc >> 24) & 1;
+    // bit-history walk
+    uint32_t b = bucket_of(k, L.logNS);
+    int live;
+    for (;;) {
+      const uint32_t kk = ovk[b];
+      if (kk == k + 1) {
+        live = ovs[b];
+        break;
+      }
+      if (kk == 0) {
+        live = s.rs[r];
+        ovk[b] = k + 1;
+        const int n = s.ovn[o];
+        s.ovl[n * kOrders + o] = (uint16_t)b;
+        s.ovn[o] = n + 1;
+        break;
+      }
+      b = (b + 1) & (uint32_t)(L.NS - 1);
+    }
+    ovs[b] = tab->nex[live][y];
+    // StateMap probability of the live state
+    uint32_t *sp = s.spl + live * kOrders + o;
+    const uint32_t v = *sp;
+    *sp = statep_next(v, y, tab->dt[v & 1023u]);
+    // mixer delta (Mixer::update, cucm_compress_v2.cu:663-678)
+    const int pr = (int)(pc & 0xffffu);
+    const int cx = (int)(pc >> 16) & 0xff;
+    const int err = ((y << 12) - pr) * 7;
+    s.dw[cx * kOrders + o] += (int)(((long long)err * s.rsmp[r]) >> 16);
+  }
+}
+
+// Unit end: overlay -> slot tables (and cleared), live probabilities become
+// frozen, deltas join the weights, the unit's bytes go out.
+__device__ inline void dec_unit_end(const DecSmem &s, const DecLayout &L, uint8_t *slot, uint8_t *out, int nbytes,
+                                    int lane) {
+  __syncwarp();
+CUCM_UNROLL
+  for (int o = 0; o < kOrders; o++) {
+    const int n = s.ovn[o];
+    uint8_t *tb = slot + table_offset(o);
+    for (int e = lane; e < n; e += 32) {
+      const int b = s.ovl[e * kOrders + o];
+      const uint32_t kk = s.ovk[o * L.NS + b];
+      tb[kk - 1] = s.ovs[o * L.NS + b];
+      s.ovk[o * L.NS + b] = 0;
+    }
+  }
+  {
+    const uint4 *src = reinterpret_cast<const uint4 *>(s.spl);
+    uint4 *dst = reinterpret_cast<uint4 *>(s.spf);
+    for (int i = lane; i < 256 * kOrders / 4; i += 32) dst[i] = src[i];
+    int4 *w4 = reinterpret_cast<int4 *>(s.w);
+    int4 *d4 = reinterpret_cast<int4 *>(s.dw);
+    for (int i = lane; i < kMixCtx * kOrders / 4; i += 32) {
+      int4 a = w4[i];
+      const int4 d = d4[i];
+      a.x += d.x;
+      a.y += d.y;
+      a.z += d.z;
+      a.w += d.w;
+      w4[i] = a;
+      d4[i] = make_int4(0, 0, 0, 0);
+    }
+  }
+  if (lane < nbytes) out[lane] = s.outb[lane];
+  __syncwarp();
+  if (lane < kOrders) s.ovn[lane] = 0;
+  __syncwarp();
+}
+
+__device__ void decompress_warp_one(const ChunkTask &t, uint8_t *slot, const DecSmem &s, const Tables *tab,
+                                    const DecLayout &L, const ModelInit *init) {
+  const int lane = threadIdx.x & 31;
+  const int U = L.U;
+  const uint64_t len = t.out_cap < t.cs ? t.out_cap : t.cs;  // bytes to decode
+  const uint64_t nbits = 8ull * len;
+  const uint8_t *pay = t.in;
+  const uint64_t plen = t.in_len;
+
+  for (int i = lane; i < 256 * kOrders; i += 32) {
+    const uint32_t v = init->statep[i & 7][i >> 3];
+    s.spf[i] = v;
+    s.spl[i] = v;
+  }
+  for (int i = lane; i < kMixCtx * kOrders; i += 32) {
+    s.w[i] = init->w[i];
+    s.dw[i] = 0;
+  }
+  for (int i = lane; i < kOrders * L.NS; i += 32) s.ovk[i] = 0;
+  if (lane < kOrders) s.ovn[lane] = 0;
+  long long wbase = dec_refill(s.win, pay, plen, 0, lane);
+
+  // coder state, identical in every lane (cucm_decompress_v2.cu:967-972)
+  uint32_t x1 = 0, x2 = 0xffffffffu, x = 0;
+  uint64_t ioff = 0;
+  for (int i = 0; i < 4; i++, ioff++) x = (x << 8) | (ioff < plen ? (uint32_t)s.win[(long long)ioff - wbase] : 255u);
+
+  // node of this lane (lanes 15..31 mirror lanes 0..14 so every gather
+  // instruction stays uniform; only lanes < 15 record)
+  const int node = lane % kDecNodes;
+  const int depth = 31 - __clz(node + 1);
+  const uint32_t pbits = (uint32_t)(node + 1 - (1 << depth));
+  const bool recorder = lane < kDecNodes;
+
+  uint64_t hist = 0;  // completed bytes, most recent in the low byte
+  uint32_t cur = 0;   // bits of the current byte
+  int r = 0;          // 0 or 4
+  int rounds_done = 0;
+
+  for (uint64_t base = 0; base < nbits; base += (uint64_t)U) {
+    const int nunit = (int)(nbits - base < (uint64_t)U ? nbits - base : (uint64_t)U);
+    const int nr = nunit >> 2;
+    int obyte = 0;
+    for (int rd = 0; rd < nr; rd++) {
+      if ((long long)ioff + 16 > wbase + kDecWin) wbase = dec_refill(s.win, pay, plen, ioff, lane);
+      // keys and gathers of this lane's node
+      const uint32_t h0 = (1u << (r + depth)) | (cur << depth) | pbits;
+      BitKeys kk;
+      bit_keys64(h0, hist, kk);
+      uint32_t st[kOrders];
+CUCM_UNROLL
+      for (int o = 0; o < kOrders; o++) st[o] = __ldcg(slot + table_offset(o) + kk.k[o]);
+      // model update of the previous round while the gathers are in flight
+      if (rd > 0 && lane < kOrders) dec_update_round(s, tab, L, lane, (rounds_done - 1) & 1);
+      // stretch, mixer context, mixer output (cucm_decompress_v2.cu:774-809)
+      const int c1 = (int)(hist & 0xffu);
+      int smp[kOrders];
+      int olen = 0;
+CUCM_UNROLL
+      for (int o = 0; o < kOrders; o++) {
+        smp[o] = tab->stretch[s.spf[st[o] * kOrders + o] >> 20];
+        olen += (smp[o] != 1);
+      }
+      const int cxt = olen + (c1 >> 5) * 10;
+      const int pr_node = mix_pr(s.w, cxt, smp, tab);
+      // decode 4 bits along the tree (cucm_decompress_v2.cu:813-868)
+      int n = 0;
+      uint32_t nib = 0;
+CUCM_UNROLL
+      for (int i = 0; i < 4; i++) {
+        const uint32_t pr = (uint32_t)__shfl_sync(0xffffffffu, pr_node, n);
+        const uint32_t xm = x1 + __umulhi(x2 - x1, pr << 20);
+        const int y = x <= xm;
+        if (y) x2 = xm; else x1 = xm + 1;
+        while ((x1 ^ x2) < 0x1000000u) {
+          x1 <<= 8;
+          x2 = (x2 << 8) | 255u;
+          x = (x << 8) | (ioff < plen ? (uint32_t)s.win[(long long)ioff - wbase] : 255u);
+          ioff++;
+        }
+        nib = (nib << 1) | (uint32_t)y;
+        n = 2 * n + 1 + y;
+      }
+      // the path's lanes record their bit for the model update
+      const int buf = rounds_done & 1;
+      if (recorder && pbits == (nib >> (4 - depth))) {
+        const int i = depth;
+        uint4 *k4 = reinterpret_cast<uint4 *>(s.rk + (buf * 4 + i) * kOrders);
+        k4[0] = make_uint4(kk.k[0], kk.k[1], kk.k[2], kk.k[3]);
+        k4[1] = make_uint4(kk.k[4], kk.k[5], kk.k[6], kk.k[7]);
+        uint2 sv;
+        sv.x = st[0] | (st[1] << 8) | (st[2] << 16) | (st[3] << 24);
+        sv.y = st[4] | (st[5] << 8) | (st[6] << 16) | (st[7] << 24);
+        *reinterpret_cast<uint2 *>(s.rs + (buf * 4 + i) * kOrders) = sv;
+        uint4 m;
+        m.x = (uint32_t)(smp[0] & 0xffff) | ((uint32_t)smp[1] << 16);
+        m.y = (uint32_t)(smp[2] & 0xffff) | ((uint32_t)smp[3] << 16);
+        m.z = (uint32_t)(smp[4] & 0xffff) | ((uint32_t)smp[5] << 16);
+        m.w = (uint32_t)(smp[6] & 0xffff) | ((uint32_t)smp[7] << 16);
+        *reinterpret_cast<uint4 *>(s.rsmp + (buf * 4 + i) * kOrders) = m;
+        s.rpc[buf * 4 + i] = (uint32_t)pr_node | ((uint32_t)cxt << 16) | (((nib >> (3 - i)) & 1u) << 24);
+      }
+      rounds_done++;
+      cur = (cur << 4) | nib;
+      r += 4;
+      if (r == 8) {
+        if (lane == 0) s.outb[obyte] = (uint8_t)cur;
+        obyte++;
+        hist = (hist << 8) | cur;
+        cur = 0;
+        r = 0;
+      }
+      __syncwarp();
+    }
+    if (lane < kOrders) dec_update_round(s, tab, L, lane, (rounds_done - 1) & 1);
+    dec_unit_end(s, L, slot, t.out + (base >> 3), nunit >> 3, lane);
+  }
+}
+
+__global__ void __launch_bounds__(kDecMaxWarps * 32)
+    decompress_warp_kernel(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
+                           const uint8_t *init_tables, const ModelInit *init, uint32_t *queue, uint32_t *status,
+                           int unit) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  const int warps = blockDim.x >> 5;
+  const DecLayout L = make_dec_layout(unit, warps);
+  Tables *tab = reinterpret_cast<Tables *>(smem_raw + L.off_tab);
+  copy_tables(&g_tables, tab);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t gw = blockIdx.x * (uint32_t)warps + (uint32_t)warp;
+  if (gw >= nslots) return;
+  const DecSmem s = carve_dec(smem_raw, L, warp);
+  uint8_t *slot = slots + (size_t)gw * kSlotTableBytes;
+  bool fresh = true;
+  for (;;) {
+    uint32_t ti = 0;
+    if (lane == 0) ti = atomicAdd(queue, 1u);
+    ti = __shfl_sync(0xffffffffu, ti, 0);
+    if (ti >= ntasks) break;
+    const ChunkTask t = tasks[ti];
+    if (t.unit != (uint32_t)unit || t.cs == 0) {
+      if (lane == 0) atomicOr(status, (uint32_t)kDevBadTask);
+      continue;
+    }
+    if (!fresh) {
+      uint4 *d = reinterpret_cast<uint4 *>(slot);
+      const size_t nv = kSlotTableBytes / 16;
+      if (init_tables) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(init_tables);
+        for (size_t i = lane; i < nv; i += 32) d[i] = src[i];
+      } else {
+        for (size_t i = lane; i < nv; i += 32) d[i] = make_uint4(0, 0, 0, 0);
+      }
+      __syncwarp();
+    }
+    fresh = false;
+    decompress_warp_one(t, slot, s, tab, L, init);
+  }
+}

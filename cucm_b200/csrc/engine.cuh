@@ -39,6 +39,7 @@ struct EngineConfig {
   int threads = 256;           // CTA size (multiple of 64)
   int spec_bits = 4;           // decoder speculation depth (1..8); never changes output
   bool generic = false;        // force the generic (non-pipelined) kernels
+  int sm_count = 0;            // SMs of the device (0 = query)
 };
 
 cudaError_t upload_tables();  // once per device (current device)
@@ -55,6 +56,8 @@ cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t
                               uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit);
 
 size_t compress_smem_bytes(int unit);
+// Chunk slots of the engine that run at once on one SM.
+int engine_slots_per_sm(bool decode, int unit, const EngineConfig &cfg);
 int compress_threads(int unit);
 size_t decompress_smem_bytes(int unit, int spec_bits);
 
