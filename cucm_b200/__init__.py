@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(_PKG, "libcucm.so")
 FORM_AUTO, FORM_PLAIN, FORM_PERSISTENT = 0, 1, 2
 
 CUCM_OK = 0
+EINVAL, ENOSPC, EFORMAT = -1, -2, -3
 _ERRORS = {
     -1: "EINVAL", -2: "ENOSPC", -3: "EFORMAT", -4: "ENOMEM", -5: "ECUDA",
     -6: "ENODEV", -7: "ETIMEOUT", -8: "EBUSY", -9: "ENOTFOUND",
@@ -82,6 +83,12 @@ SIGNATURES = [
     ("cucm_decompress_many", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), _u64p,
                                             ctypes.POINTER(ctypes.c_void_p), _u64p, _u64p,
                                             ctypes.POINTER(ctypes.c_int)]),
+    ("cucm_compress_many_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
+                                              _u64p, ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p), _u64p,
+                                              _u64p, ctypes.POINTER(ctypes.c_int)]),
+    ("cucm_decompress_many_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
+                                                _u64p, ctypes.POINTER(ctypes.c_void_p), _u64p, _u64p,
+                                                ctypes.POINTER(ctypes.c_int)]),
     ("cucm_last_device_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("cucm_last_launches", ctypes.c_int, [ctypes.c_void_p, _u64p]),
     ("cucm_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
@@ -116,6 +123,16 @@ def default_params(chunksize=None, unit=None, prelearn=None, batch=None):
     if batch is not None:
         p.batch = int(batch)
     return p
+
+
+def many_cap(n, chunksize, prelearn=0):
+    """An output capacity that nearly every container of n input bytes fits:
+    up to 2x plus 4 KiB per chunk.  A chunk shorter than the chunk size still
+    codes the stale model buffer up to the chunk end, as the reference does,
+    so even a tiny input can need about a chunk's worth.  The batched calls
+    redo the rare container that needs more."""
+    nchunks = (max(n - prelearn, 0) + chunksize - 1) // chunksize
+    return 64 + prelearn * 8 + nchunks * (8 + 2 * chunksize + 4096)
 
 
 def _buf(data):
@@ -225,21 +242,32 @@ class Context:
         return out.raw[:out_size]
 
     def compress_many(self, buffers, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+        """Containers of many buffers in one call (the batched form); each is
+        byte-identical to compress() of that buffer alone."""
         p = default_params(chunksize, unit, prelearn, batch)
         k = len(buffers)
         bufs = [_buf(b) for b in buffers]
         ins = (ctypes.c_void_p * k)(*[b[0] for b in bufs])
         ns = (ctypes.c_uint64 * k)(*[b[1] for b in bufs])
-        caps = [lib().cucm_compress_bound(b[1], ctypes.byref(p)) for b in bufs]
+        # optimistic output sizes; entries that need more are redone alone
+        caps = [min(lib().cucm_compress_bound(b[1], ctypes.byref(p)), many_cap(b[1], chunksize)) for b in bufs]
         outs_b = [ctypes.create_string_buffer(max(c, 1)) for c in caps]
         outs = (ctypes.c_void_p * k)(*[ctypes.addressof(o) for o in outs_b])
         capa = (ctypes.c_uint64 * k)(*caps)
         got = (ctypes.c_uint64 * k)()
         st = (ctypes.c_int * k)()
         rc = lib().cucm_compress_many(self._h, k, ins, ns, ctypes.byref(p), outs, capa, got, st)
-        if rc:
+        res = []
+        for i in range(k):
+            if st[i] == ENOSPC:
+                res.append(self.compress(buffers[i], chunksize, unit, prelearn, batch))
+            elif st[i]:
+                raise CucmError(st[i], "cucm_compress_many")
+            else:
+                res.append(outs_b[i].raw[:got[i]])
+        if rc and rc != ENOSPC:
             raise CucmError(rc, "cucm_compress_many")
-        return [outs_b[i].raw[:got[i]] for i in range(k)]
+        return res
 
     def decompress_many(self, blobs):
         k = len(blobs)
@@ -262,6 +290,32 @@ class Context:
         if rc:
             raise CucmError(rc, "cucm_decompress_many")
         return [outs_b[i].raw[:got[i]] for i in range(k)]
+
+    def compress_many_dev(self, ins, outs, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+        """Batched form on device buffers.  ins: [(device ptr, bytes)],
+        outs: [(device ptr, capacity)].  Returns (sizes, statuses)."""
+        p = default_params(chunksize, unit, prelearn, batch)
+        return self._many_dev(lib().cucm_compress_many_dev, ins, outs, ctypes.byref(p))
+
+    def decompress_many_dev(self, ins, outs):
+        """Batched decompression on device buffers; see compress_many_dev."""
+        return self._many_dev(lib().cucm_decompress_many_dev, ins, outs, None)
+
+    def _many_dev(self, fn, ins, outs, params):
+        k = len(ins)
+        a_in = (ctypes.c_void_p * k)(*[int(x[0]) for x in ins])
+        a_n = (ctypes.c_uint64 * k)(*[int(x[1]) for x in ins])
+        a_out = (ctypes.c_void_p * k)(*[int(x[0]) for x in outs])
+        a_cap = (ctypes.c_uint64 * k)(*[int(x[1]) for x in outs])
+        got = (ctypes.c_uint64 * k)()
+        st = (ctypes.c_int * k)()
+        if params is None:
+            rc = fn(self._h, k, a_in, a_n, a_out, a_cap, got, st)
+        else:
+            rc = fn(self._h, k, a_in, a_n, params, a_out, a_cap, got, st)
+        if rc and rc != ENOSPC:
+            raise CucmError(rc, fn.__name__)
+        return list(got), list(st)
 
     def last_device_ms(self):
         v = ctypes.c_double()

@@ -30,93 +30,7 @@ using namespace cucm;
 
 namespace {
 
-constexpr uint64_t kHeaderBytes = 21;
-
-// ---------------------------------------------------------------------------
-// Pack kernel: one CTA per chunk copies its payload from scratch into the
-// container, writes its big-endian end offset, and the first chunk of a batch
-// writes the batch's little-endian size field.
-struct PackEntry {
-  uint64_t src;        // scratch offset of the payload
-  uint64_t dst;        // container offset of the payload
-  uint64_t len;        // payload bytes
-  uint64_t table_at;   // container offset of this chunk's end-offset field
-  uint32_t end_value;  // big-endian field value
-  uint32_t batch_size; // valid when size_at != ~0
-  uint64_t size_at;    // container offset of the batch size field or ~0
-};
-
-__global__ void pack_kernel(const PackEntry *e, uint32_t n, const uint8_t *scratch, uint8_t *dst) {
-  const uint32_t k = blockIdx.x;
-  if (k >= n) return;
-  const PackEntry p = e[k];
-  const uint8_t *s = scratch + p.src;
-  uint8_t *d = dst + p.dst;
-  for (uint64_t i = threadIdx.x; i < p.len; i += blockDim.x) d[i] = s[i];
-  if (threadIdx.x == 0) {
-    uint8_t *t = dst + p.table_at;
-    t[0] = (uint8_t)(p.end_value >> 24);
-    t[1] = (uint8_t)(p.end_value >> 16);
-    t[2] = (uint8_t)(p.end_value >> 8);
-    t[3] = (uint8_t)p.end_value;
-    if (p.size_at != ~0ull) {
-      uint8_t *z = dst + p.size_at;
-      z[0] = (uint8_t)p.batch_size;
-      z[1] = (uint8_t)(p.batch_size >> 8);
-      z[2] = (uint8_t)(p.batch_size >> 16);
-      z[3] = (uint8_t)(p.batch_size >> 24);
-    }
-  }
-}
-
-struct DevBuf {
-  void *p = nullptr;
-  size_t cap = 0;
-  ~DevBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-  }
-  cudaError_t ensure(size_t n) {
-    if (n <= cap) return cudaSuccess;
-    release();
-    size_t want = n < 256 ? 256 : n;
-    cudaError_t e = cudaMalloc(&p, want);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      return e;
-    }
-    cap = want;
-    return cudaSuccess;
-  }
-  template <typename T>
-  T *as() const {
-    return reinterpret_cast<T *>(p);
-  }
-};
-
-inline void put_be32(uint8_t *p, uint32_t v) {
-  p[0] = (uint8_t)(v >> 24);
-  p[1] = (uint8_t)(v >> 16);
-  p[2] = (uint8_t)(v >> 8);
-  p[3] = (uint8_t)v;
-}
-inline uint32_t get_be32(const uint8_t *p) {
-  return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3];
-}
-inline uint32_t get_le32(const uint8_t *p) {
-  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
-}
-
-uint64_t scratch_cap(uint64_t cs) {
-  // Typical payloads stay below ~1.1x the chunk; 2x + 4 KiB leaves margin.
-  // A chunk that still overflows is re-coded with the hard bound.
-  uint64_t c = 2 * cs + 4096;
-  uint64_t hard = 32 * cs + 16;
-  return ((c < hard ? c : hard) + 15) & ~15ull;
-}
-uint64_t hard_cap(uint64_t cs) { return (32 * cs + 1 + 15) & ~15ull; }
+#include "container.cuh"
 
 }  // namespace
 
@@ -131,7 +45,7 @@ struct cucm_ctx {
   uint32_t nslots = 0;
   DevBuf image;    // prelearned slot image (when used)
   DevBuf d_init;   // ModelInit
-  DevBuf d_tasks, d_results, d_queue, d_status, d_scratch, d_pack, d_body, d_out;
+  DevBuf d_tasks, d_results, d_queue, d_status, d_scratch, d_big, d_pack, d_body, d_out;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around the engine launches
   double last_ms = 0.0;
@@ -351,250 +265,128 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
   return CUCM_OK;
 }
 
-// Validate stream parameters the way the reference's container can hold them.
-int check_params(const cucm_params *p, uint64_t n) {
-  if (!p) return CUCM_EINVAL;
-  if (p->chunksize == 0 || p->chunksize > 0xffffffffull) return CUCM_EINVAL;
-  if (p->unit < 32 || p->unit > (uint32_t)kMaxUnit || p->unit % 32) return CUCM_EINVAL;
-  if (p->batch == 0 || p->batch > 0xffff) return CUCM_EINVAL;
-  if (p->prelearn > n) return CUCM_EINVAL;
-  if (n > 0xffffffffull) return CUCM_EINVAL;  // header field is 32 bits
-  return CUCM_OK;
-}
-
-struct Layout2 {
-  uint64_t nchunks, nbatches, total;
-  std::vector<uint64_t> lens;
+// A run of input bytes in device memory coded as consecutive chunks.
+struct Seg {
+  const uint8_t *d_in;
+  uint64_t n;
 };
 
-// Encode every chunk of `d_body[0..n)` and pack the batches at d_dst.
-// Returns the container body size (everything after the prelearn block).
-int encode_and_pack(cucm_ctx *c, const uint8_t *d_body, uint64_t n, uint64_t cs, uint32_t unit, uint32_t batch,
-                    const ModelSource &ms, bool with_sizes, uint8_t *d_dst, uint64_t dst_cap, uint64_t *body_n,
-                    std::vector<uint64_t> *lens_out) {
-  const uint64_t nchunks = (n + cs - 1) / cs;
-  *body_n = 0;
+// Chunk payloads of one engine run over several segments.
+struct Encoded {
+  std::vector<uint64_t> first;        // first chunk of each segment, plus the total
+  std::vector<uint64_t> lens;         // payload bytes per chunk
+  std::vector<const uint8_t *> src;   // payload location per chunk (device)
+};
+
+// Code every chunk of every segment in one engine run.  Payloads land in an
+// optimistic scratch slot per chunk; chunks that overflow it are coded again
+// with the hard bound.
+int encode_chunks(cucm_ctx *c, const std::vector<Seg> &segs, uint64_t cs, uint32_t unit, const ModelSource &ms,
+                  uint64_t other_bytes, Encoded &e) {
+  e.first.assign(1, 0);
+  for (const Seg &g : segs) e.first.push_back(e.first.back() + (g.n + cs - 1) / cs);
+  const uint64_t nchunks = e.first.back();
+  e.lens.assign(nchunks, 0);
+  e.src.assign(nchunks, nullptr);
   if (nchunks == 0) return CUCM_OK;
-  std::vector<uint64_t> scap(nchunks), soff(nchunks);
-  uint64_t tot = 0;
-  for (uint64_t k = 0; k < nchunks; k++) {
-    scap[k] = scratch_cap(cs);
-    soff[k] = tot;
-    tot += scap[k];
-  }
-  CK(c->d_scratch.ensure(tot));
+  const uint64_t scap = scratch_cap(cs);
+  CK(c->d_scratch.ensure(scap * nchunks));
   CK(c->d_results.ensure(sizeof(uint64_t) * nchunks));
   std::vector<ChunkTask> tasks(nchunks);
-  for (uint64_t k = 0; k < nchunks; k++) {
-    ChunkTask &t = tasks[k];
-    t.in = d_body + k * cs;
-    t.in_len = std::min<uint64_t>(cs, n - k * cs);
-    t.out = c->d_scratch.as<uint8_t>() + soff[k];
-    t.out_cap = scap[k];
-    t.cs = (uint32_t)cs;
-    t.unit = unit;
-    t.result = c->d_results.as<uint64_t>() + k;
-  }
-  uint64_t other = tot + c->d_body.cap + c->d_out.cap;
-  int rc = run_engine(c, false, tasks, (int)unit, ms, other);
-  if (rc) return rc;
-  std::vector<uint64_t> lens(nchunks);
-  uint32_t status = 0;
-  CK(cudaMemcpyAsync(lens.data(), c->d_results.p, sizeof(uint64_t) * nchunks, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(&status, c->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  if (status & kDevBadTask) return CUCM_EINVAL;
-  // Re-code chunks whose payload overflowed the optimistic scratch.
-  std::vector<uint64_t> redo;
-  for (uint64_t k = 0; k < nchunks; k++)
-    if (lens[k] > scap[k]) redo.push_back(k);
-  DevBuf big;
-  std::vector<uint64_t> big_off(nchunks, ~0ull);
-  if (!redo.empty()) {
-    uint64_t btot = 0;
-    for (uint64_t k : redo) {
-      big_off[k] = btot;
-      btot += hard_cap(cs);
-    }
-    CK(big.ensure(btot));
-    std::vector<ChunkTask> rt;
-    for (uint64_t k : redo) {
-      ChunkTask t = tasks[0];
-      t.in = d_body + k * cs;
-      t.in_len = std::min<uint64_t>(cs, n - k * cs);
-      t.out = big.as<uint8_t>() + big_off[k];
-      t.out_cap = hard_cap(cs);
+  for (size_t g = 0; g < segs.size(); g++) {
+    for (uint64_t k = e.first[g]; k < e.first[g + 1]; k++) {
+      const uint64_t j = k - e.first[g];
+      ChunkTask &t = tasks[k];
+      t.in = segs[g].d_in + j * cs;
+      t.in_len = std::min<uint64_t>(cs, segs[g].n - j * cs);
+      t.out = c->d_scratch.as<uint8_t>() + k * scap;
+      t.out_cap = scap;
       t.cs = (uint32_t)cs;
       t.unit = unit;
       t.result = c->d_results.as<uint64_t>() + k;
-      rt.push_back(t);
     }
-    rc = run_engine(c, false, rt, (int)unit, ms, other + btot);
+  }
+  const std::vector<ChunkTask> orig = tasks;
+  const uint64_t other = other_bytes + scap * nchunks;
+  int rc = run_engine(c, false, tasks, (int)unit, ms, other);
+  if (rc) return rc;
+  uint32_t status = 0;
+  CK(cudaMemcpyAsync(e.lens.data(), c->d_results.p, sizeof(uint64_t) * nchunks, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&status, c->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (status & kDevBadTask) return CUCM_EINVAL;
+  for (uint64_t k = 0; k < nchunks; k++) e.src[k] = orig[k].out;
+  std::vector<uint64_t> redo;
+  for (uint64_t k = 0; k < nchunks; k++)
+    if (e.lens[k] > scap) redo.push_back(k);
+  if (!redo.empty()) {
+    const uint64_t hc = hard_cap(cs);
+    CK(c->d_big.ensure(hc * redo.size()));
+    std::vector<ChunkTask> rt;
+    for (size_t i = 0; i < redo.size(); i++) {
+      ChunkTask t = orig[redo[i]];
+      t.out = c->d_big.as<uint8_t>() + i * hc;
+      t.out_cap = hc;
+      rt.push_back(t);
+      e.src[redo[i]] = t.out;
+    }
+    rc = run_engine(c, false, rt, (int)unit, ms, other + hc * redo.size());
     if (rc) return rc;
-    CK(cudaMemcpyAsync(lens.data(), c->d_results.p, sizeof(uint64_t) * nchunks, cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(e.lens.data(), c->d_results.p, sizeof(uint64_t) * nchunks, cudaMemcpyDeviceToHost,
                        c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (uint64_t k : redo)
-      if (lens[k] > hard_cap(cs)) return CUCM_ECUDA;
+      if (e.lens[k] > hc) return CUCM_ECUDA;
   }
-  // Layout of the batches (cudaencodefinal, cucm_compress_v2.cu:880-914).
-  const uint64_t nb = (nchunks + batch - 1) / batch;
-  std::vector<PackEntry> pe(nchunks);
-  uint64_t w = 0;
-  for (uint64_t b = 0; b < nb; b++) {
-    uint64_t k0 = b * batch, k1 = std::min<uint64_t>(k0 + batch, nchunks), C = k1 - k0;
-    uint64_t bsz = 4 * C;
-    for (uint64_t k = k0; k < k1; k++) bsz += lens[k];
-    uint64_t size_at = w;
-    if (with_sizes) w += 4;
-    uint64_t table = w;
-    w += 4 * C;
-    uint64_t acc = 4 * C - 1;
-    for (uint64_t k = k0; k < k1; k++) {
-      acc += lens[k];
-      PackEntry &p = pe[k];
-      bool in_big = big_off[k] != ~0ull;
-      p.src = in_big ? big_off[k] : soff[k];
-      p.dst = w;
-      p.len = lens[k];
-      p.table_at = table + 4 * (k - k0);
-      p.end_value = (uint32_t)acc;
-      p.size_at = (k == k0 && with_sizes) ? size_at : ~0ull;
-      p.batch_size = (uint32_t)bsz;
-      w += lens[k];
-    }
-  }
-  if (w > dst_cap) return CUCM_ENOSPC;
-  CK(c->d_pack.ensure(sizeof(PackEntry) * nchunks));
-  CK(cudaMemcpyAsync(c->d_pack.p, pe.data(), sizeof(PackEntry) * nchunks, cudaMemcpyHostToDevice, c->stream));
-  if (redo.empty()) {
-    pack_kernel<<<(unsigned)nchunks, 256, 0, c->stream>>>(c->d_pack.as<PackEntry>(), (uint32_t)nchunks,
-                                                           c->d_scratch.as<uint8_t>(), d_dst);
-    c->launches += 1;
-  } else {
-    // two sources: pack the overflowed chunks from the big scratch separately
-    std::vector<PackEntry> a, bb;
-    for (uint64_t k = 0; k < nchunks; k++) (big_off[k] != ~0ull ? bb : a).push_back(pe[k]);
-    DevBuf pa, pb;
-    CK(pa.ensure(sizeof(PackEntry) * std::max<size_t>(a.size(), 1)));
-    CK(pb.ensure(sizeof(PackEntry) * std::max<size_t>(bb.size(), 1)));
-    CK(cudaMemcpyAsync(pa.p, a.data(), sizeof(PackEntry) * a.size(), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(pb.p, bb.data(), sizeof(PackEntry) * bb.size(), cudaMemcpyHostToDevice, c->stream));
-    if (!a.empty())
-      pack_kernel<<<(unsigned)a.size(), 256, 0, c->stream>>>(pa.as<PackEntry>(), (uint32_t)a.size(),
-                                                             c->d_scratch.as<uint8_t>(), d_dst);
-    pack_kernel<<<(unsigned)bb.size(), 256, 0, c->stream>>>(pb.as<PackEntry>(), (uint32_t)bb.size(),
-                                                            big.as<uint8_t>(), d_dst);
-    c->launches += 2;
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(c->stream));
-  }
+  return CUCM_OK;
+}
+
+// Body layout of segment g's chunks (see layout_chunks).
+uint64_t layout_body(const Encoded &e, size_t g, uint32_t batch, bool with_sizes, uint8_t *base,
+                     std::vector<PackEntry> *pe) {
+  const uint64_t f = e.first[g];
+  return layout_chunks(e.lens.data() + f, e.src.data() + f, e.first[g + 1] - f, batch, with_sizes, base, pe);
+}
+
+// One launch packs every laid-out body.
+int pack_bodies(cucm_ctx *c, const std::vector<PackEntry> &pe) {
+  if (pe.empty()) return CUCM_OK;
+  CK(c->d_pack.ensure(sizeof(PackEntry) * pe.size()));
+  CK(cudaMemcpyAsync(c->d_pack.p, pe.data(), sizeof(PackEntry) * pe.size(), cudaMemcpyHostToDevice, c->stream));
+  pack_kernel<<<(unsigned)pe.size(), 256, 0, c->stream>>>(c->d_pack.as<PackEntry>(), (uint32_t)pe.size());
   CK(cudaGetLastError());
-  *body_n = w;
-  if (lens_out) *lens_out = lens;
+  c->launches += 1;
   return CUCM_OK;
 }
 
-// Container header + prelearn block.  Also produces the initial model.
-int make_header(const uint8_t *in, uint64_t n, const cucm_params *p, std::vector<uint8_t> &hdr,
-                std::unique_ptr<HostModel> &hm) {
-  std::vector<uint8_t> pl;
-  uint64_t coded = 0;
-  if (p->prelearn > 0) {
-    hm.reset(new HostModel());
-    coded = hm->prelearn_encode(in, p->prelearn, pl);
-  }
-  const bool raw = p->prelearn <= coded;  // cucm_compress_v2.cu:1217-1223
-  const uint64_t pl_len = raw ? p->prelearn : coded;
-  hdr.assign(kHeaderBytes + pl_len, 0);
-  put_be32(&hdr[0], (uint32_t)n);
-  hdr[4] = (uint8_t)(p->batch >> 8);
-  hdr[5] = (uint8_t)p->batch;
-  hdr[6] = (uint8_t)(p->unit >> 8);
-  hdr[7] = (uint8_t)p->unit;
-  put_be32(&hdr[8], (uint32_t)p->chunksize);
-  put_be32(&hdr[12], (uint32_t)coded);
-  put_be32(&hdr[16], (uint32_t)p->prelearn);
-  hdr[20] = raw ? 0 : 1;
-  if (pl_len) std::memcpy(&hdr[kHeaderBytes], raw ? in : pl.data(), pl_len);
-  return CUCM_OK;
-}
-
-struct Parsed {
-  uint64_t total, cs, prelearn, pl_coded, pl_len;
-  uint32_t batch, unit;
-  int coded;
+// Chunks of one container to decode: payload extents in device memory and
+// where its output bytes go.
+struct DecJob {
+  const uint8_t *d_body;
+  std::vector<uint64_t> off, len;
+  uint64_t total, cs;
+  uint8_t *d_out;
 };
 
-int parse_header(const uint8_t *in, uint64_t n, Parsed &h) {
-  if (!in || n < kHeaderBytes) return CUCM_EFORMAT;
-  h.total = get_be32(in);
-  h.batch = ((uint32_t)in[4] << 8) | in[5];
-  h.unit = ((uint32_t)in[6] << 8) | in[7];
-  h.cs = get_be32(in + 8);
-  h.pl_coded = get_be32(in + 12);
-  h.prelearn = get_be32(in + 16);
-  h.coded = in[20];
-  if (h.cs == 0 || h.batch == 0 || h.unit < 32 || h.unit > (uint32_t)kMaxUnit || h.unit % 32) return CUCM_EFORMAT;
-  if (h.prelearn > h.total) return CUCM_EFORMAT;
-  h.pl_len = h.coded ? h.pl_coded : h.prelearn;
-  if (kHeaderBytes + h.pl_len > n) return CUCM_EFORMAT;
-  return CUCM_OK;
-}
-
-// Chunk payload extents of the batches that follow the prelearn block
-// (cucm_decompress_v2.cu:1223-1237).  Offsets are relative to `body`.
-int parse_batches(const uint8_t *body, uint64_t body_n, uint64_t nchunks, uint32_t batch, bool with_sizes,
-                  std::vector<uint64_t> &off, std::vector<uint64_t> &len) {
-  off.resize(nchunks);
-  len.resize(nchunks);
-  uint64_t r = 0;
-  const uint64_t nb = (nchunks + batch - 1) / batch;
-  for (uint64_t b = 0; b < nb; b++) {
-    uint64_t k0 = b * batch, k1 = std::min<uint64_t>(k0 + batch, nchunks), C = k1 - k0;
-    uint64_t bsz;
-    if (with_sizes) {
-      if (r + 4 > body_n) return CUCM_EFORMAT;
-      bsz = get_le32(body + r);
-      r += 4;
-    } else {
-      bsz = body_n - r;
+// Decode every chunk of every job in one engine run.
+int decode_jobs(cucm_ctx *c, const std::vector<DecJob> &jobs, uint32_t unit, const ModelSource &ms,
+                uint64_t other_bytes) {
+  std::vector<ChunkTask> tasks;
+  for (const DecJob &j : jobs) {
+    for (uint64_t k = 0; k < j.off.size(); k++) {
+      ChunkTask t;
+      t.in = j.d_body + j.off[k];
+      t.in_len = j.len[k];
+      t.out = j.d_out + k * j.cs;
+      t.out_cap = std::min<uint64_t>(j.cs, j.total - k * j.cs);
+      t.cs = (uint32_t)j.cs;
+      t.unit = unit;
+      t.result = nullptr;
+      tasks.push_back(t);
     }
-    if (bsz < 4 * C || r + bsz > body_n) return CUCM_EFORMAT;
-    const uint64_t pay0 = r + 4 * C;
-    const uint64_t pay_n = bsz - 4 * C;
-    uint64_t start = 0;
-    for (uint64_t k = k0; k < k1; k++) {
-      uint64_t endv = get_be32(body + r + 4 * (k - k0));
-      if (endv + 1 < 4 * C) return CUCM_EFORMAT;
-      uint64_t end = endv + 1 - 4 * C;
-      if (end < start || end > pay_n) return CUCM_EFORMAT;
-      off[k] = pay0 + start;
-      len[k] = end - start;
-      start = end;
-    }
-    r += bsz;
   }
-  return CUCM_OK;
-}
-
-int decode_chunks(cucm_ctx *c, const uint8_t *d_body, const std::vector<uint64_t> &off,
-                  const std::vector<uint64_t> &len, uint64_t total, uint64_t cs, uint32_t unit, const ModelSource &ms,
-                  uint8_t *d_out) {
-  const uint64_t nchunks = off.size();
-  if (nchunks == 0) return CUCM_OK;
-  std::vector<ChunkTask> tasks(nchunks);
-  for (uint64_t k = 0; k < nchunks; k++) {
-    ChunkTask &t = tasks[k];
-    t.in = d_body + off[k];
-    t.in_len = len[k];
-    t.out = d_out + k * cs;
-    t.out_cap = std::min<uint64_t>(cs, total - k * cs);
-    t.cs = (uint32_t)cs;
-    t.unit = unit;
-    t.result = nullptr;
-  }
-  int rc = run_engine(c, true, tasks, (int)unit, ms, c->d_body.cap + c->d_out.cap);
+  if (tasks.empty()) return CUCM_OK;
+  int rc = run_engine(c, true, tasks, (int)unit, ms, other_bytes);
   if (rc) return rc;
   uint32_t status = 0;
   CK(cudaMemcpyAsync(&status, c->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
@@ -698,169 +490,290 @@ int cucm_decompressed_size(const uint8_t *in, uint64_t n, uint64_t *size) {
   return CUCM_OK;
 }
 
-static int compress_impl(cucm_ctx *c, const uint8_t *in, uint64_t n, const cucm_params *p, uint8_t *out,
-                         uint64_t cap, uint64_t *out_n, bool dev) {
-  if (!c || !out_n || (!in && n) || !out) return CUCM_EINVAL;
-  int rc = check_params(p, n);
-  if (rc) return rc;
+// Compress `count` containers that share the stream parameters `p` (the
+// whole of compress_file, cucm_compress_v2.cu:1151-1250, per container).
+// Containers without a prelearn prefix all start from the zero model and are
+// coded in ONE engine run over all their chunks; a prelearn prefix gives a
+// container its own initial model and so its own run.  `dev`: ins and outs
+// are device buffers.
+static int compress_containers(cucm_ctx *c, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                               const cucm_params *p, uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns,
+                               int *status, bool dev) {
   std::lock_guard<std::mutex> g(c->mu);
   CK(cudaSetDevice(c->device));
-  // The prelearn prefix is read on the host (it is host work in the reference).
-  std::vector<uint8_t> pre;
-  const uint8_t *pre_ptr = in;
-  if (dev && p->prelearn) {
-    pre.resize(p->prelearn);
-    CK(cudaMemcpy(pre.data(), in, p->prelearn, cudaMemcpyDeviceToHost));
-    pre_ptr = pre.data();
+  std::vector<std::vector<uint8_t>> hdrs(count);
+  std::vector<std::unique_ptr<HostModel>> models(count);
+  std::vector<uint32_t> ok;
+  for (uint32_t i = 0; i < count; i++) {
+    out_ns[i] = 0;
+    status[i] = check_params(p, ns[i]);
+    if (!status[i] && ((!ins[i] && ns[i]) || !outs[i])) status[i] = CUCM_EINVAL;
+    if (status[i]) continue;
+    // The prelearn prefix is read on the host (it is host work in the reference).
+    std::vector<uint8_t> pre;
+    const uint8_t *pre_ptr = ins[i];
+    if (dev && p->prelearn) {
+      pre.resize(p->prelearn);
+      CK(cudaMemcpy(pre.data(), ins[i], p->prelearn, cudaMemcpyDeviceToHost));
+      pre_ptr = pre.data();
+    }
+    status[i] = make_header(pre_ptr, ns[i], p, hdrs[i], models[i]);
+    if (!status[i] && caps[i] < hdrs[i].size()) {
+      status[i] = CUCM_ENOSPC;
+      out_ns[i] = hdrs[i].size();
+    }
+    if (!status[i]) ok.push_back(i);
   }
-  std::vector<uint8_t> hdr;
-  std::unique_ptr<HostModel> hm;
-  rc = make_header(pre_ptr, n, p, hdr, hm);
-  if (rc) return rc;
-  ModelSource ms;
-  std::vector<uint8_t> image;
-  if (hm) {
-    hm->to_device(image, ms.init);
-    ms.image = &image;
+  std::vector<std::vector<uint32_t>> groups;
+  if (p->prelearn == 0) {
+    if (!ok.empty()) groups.push_back(ok);
   } else {
-    zero_model(ms.init);
+    for (uint32_t i : ok) groups.push_back({i});
   }
-  const uint64_t body_in = n - p->prelearn;
-  const uint64_t hl = hdr.size();
-  if (cap < hl) return CUCM_ENOSPC;
   timing_begin(c);
-  const uint8_t *d_body;
-  uint8_t *d_dst;
-  uint64_t dst_cap;
-  if (dev) {
-    d_body = in + p->prelearn;
-    d_dst = out + hl;
-    dst_cap = cap - hl;
-  } else {
-    CK(c->d_body.ensure(body_in ? body_in : 1));
-    if (body_in)
-      CK(cudaMemcpyAsync(c->d_body.p, in + p->prelearn, body_in, cudaMemcpyHostToDevice, c->stream));
-    d_body = c->d_body.as<uint8_t>();
-    uint64_t nchunks = (body_in + p->chunksize - 1) / p->chunksize;
-    uint64_t est = body_in * 2 + nchunks * (8 + 4096) + 64;
-    CK(c->d_out.ensure(est));
-    d_dst = c->d_out.as<uint8_t>();
-    dst_cap = c->d_out.cap;
-  }
-  uint64_t body_n = 0;
-  rc = encode_and_pack(c, d_body, body_in, p->chunksize, p->unit, p->batch, ms, true, d_dst, dst_cap, &body_n,
-                       nullptr);
-  if (rc == CUCM_ENOSPC && !dev) {
-    // grow the device staging buffer to the hard bound and retry
-    CK(c->d_out.ensure(cucm_compress_bound(n, p)));
-    rc = encode_and_pack(c, d_body, body_in, p->chunksize, p->unit, p->batch, ms, true, c->d_out.as<uint8_t>(),
-                         c->d_out.cap, &body_n, nullptr);
-  }
-  if (rc) {
-    timing_end(c);
-    return rc;
-  }
-  if (hl + body_n > cap) {
-    timing_end(c);
-    return CUCM_ENOSPC;
-  }
-  if (dev) {
-    CK(cudaMemcpyAsync(out, hdr.data(), hl, cudaMemcpyHostToDevice, c->stream));
-  } else {
-    std::memcpy(out, hdr.data(), hl);
-    if (body_n) CK(cudaMemcpyAsync(out + hl, c->d_out.p, body_n, cudaMemcpyDeviceToHost, c->stream));
+  int rc = CUCM_OK;
+  for (const std::vector<uint32_t> &grp : groups) {
+    ModelSource ms;
+    std::vector<uint8_t> image;
+    if (models[grp[0]]) {
+      models[grp[0]]->to_device(image, ms.init);
+      ms.image = &image;
+    } else {
+      zero_model(ms.init);
+    }
+    std::vector<Seg> segs;
+    if (dev) {
+      for (uint32_t i : grp) segs.push_back({ins[i] + p->prelearn, ns[i] - p->prelearn});
+    } else {
+      uint64_t tot = 0;
+      std::vector<uint64_t> at;
+      for (uint32_t i : grp) {
+        at.push_back(tot);
+        tot += ((ns[i] - p->prelearn) + 15) & ~15ull;
+      }
+      CK(c->d_body.ensure(tot ? tot : 1));
+      for (size_t j = 0; j < grp.size(); j++) {
+        const uint32_t i = grp[j];
+        const uint64_t bn = ns[i] - p->prelearn;
+        if (bn)
+          CK(cudaMemcpyAsync(c->d_body.as<uint8_t>() + at[j], ins[i] + p->prelearn, bn, cudaMemcpyHostToDevice,
+                             c->stream));
+        segs.push_back({c->d_body.as<uint8_t>() + at[j], bn});
+      }
+    }
+    Encoded e;
+    rc = encode_chunks(c, segs, p->chunksize, p->unit, ms, c->d_body.cap + c->d_out.cap, e);
+    if (rc) break;
+    std::vector<uint64_t> body(grp.size()), at(grp.size());
+    uint64_t stage = 0;
+    for (size_t j = 0; j < grp.size(); j++) {
+      const uint32_t i = grp[j];
+      body[j] = layout_body(e, j, p->batch, true, nullptr, nullptr);
+      out_ns[i] = hdrs[i].size() + body[j];
+      if (out_ns[i] > caps[i]) status[i] = CUCM_ENOSPC;
+      at[j] = stage;
+      stage += (body[j] + 15) & ~15ull;
+    }
+    if (!dev) CK(c->d_out.ensure(stage ? stage : 1));
+    std::vector<PackEntry> pe;
+    for (size_t j = 0; j < grp.size(); j++) {
+      const uint32_t i = grp[j];
+      if (status[i]) continue;
+      uint8_t *base = dev ? outs[i] + hdrs[i].size() : c->d_out.as<uint8_t>() + at[j];
+      layout_body(e, j, p->batch, true, base, &pe);
+    }
+    rc = pack_bodies(c, pe);
+    if (rc) break;
+    for (size_t j = 0; j < grp.size(); j++) {
+      const uint32_t i = grp[j];
+      if (status[i]) continue;
+      const uint64_t hl = hdrs[i].size();
+      if (dev) {
+        CK(cudaMemcpyAsync(outs[i], hdrs[i].data(), hl, cudaMemcpyHostToDevice, c->stream));
+      } else {
+        std::memcpy(outs[i], hdrs[i].data(), hl);
+        if (body[j])
+          CK(cudaMemcpyAsync(outs[i] + hl, c->d_out.as<uint8_t>() + at[j], body[j], cudaMemcpyDeviceToHost,
+                             c->stream));
+      }
+    }
+    CK(cudaStreamSynchronize(c->stream));
   }
   timing_end(c);
   CK(cudaStreamSynchronize(c->stream));
-  *out_n = hl + body_n;
+  if (rc) {
+    for (uint32_t i : ok)
+      if (!status[i]) status[i] = rc;
+    return rc;
+  }
+  for (uint32_t i = 0; i < count; i++)
+    if (status[i]) return status[i];
   return CUCM_OK;
 }
 
 int cucm_compress(cucm_ctx *c, const uint8_t *in, uint64_t n, const cucm_params *p, uint8_t *out, uint64_t cap,
                   uint64_t *out_n) {
-  return compress_impl(c, in, n, p, out, cap, out_n, false);
+  if (!c || !out_n || !p) return CUCM_EINVAL;
+  int st = 0;
+  return compress_containers(c, 1, &in, &n, p, &out, &cap, out_n, &st, false);
 }
 
 int cucm_compress_dev(cucm_ctx *c, const uint8_t *in, uint64_t n, const cucm_params *p, uint8_t *out, uint64_t cap,
                       uint64_t *out_n) {
-  return compress_impl(c, in, n, p, out, cap, out_n, true);
+  if (!c || !out_n || !p) return CUCM_EINVAL;
+  int st = 0;
+  return compress_containers(c, 1, &in, &n, p, &out, &cap, out_n, &st, true);
 }
 
-static int decompress_impl(cucm_ctx *c, const uint8_t *in, uint64_t n, uint8_t *out, uint64_t cap,
-                           uint64_t *out_n, bool dev) {
-  if (!c || !in || !out_n) return CUCM_EINVAL;
+// Decompress `count` containers (decompress, cucm_decompress_v2.cu:1185-1248,
+// per container).  Containers without a prelearn prefix are decoded in one
+// engine run per unit length; a prelearn prefix means its own model and run.
+static int decompress_containers(cucm_ctx *c, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                                 uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns, int *status, bool dev) {
   std::lock_guard<std::mutex> g(c->mu);
   CK(cudaSetDevice(c->device));
   // The header, prelearn block and batch framing are parsed on the host.
-  std::vector<uint8_t> host_copy;
-  const uint8_t *h = in;
-  if (dev) {
-    host_copy.resize(n);
-    CK(cudaMemcpy(host_copy.data(), in, n, cudaMemcpyDeviceToHost));
-    h = host_copy.data();
-  }
-  Parsed ph;
-  int rc = parse_header(h, n, ph);
-  if (rc) return rc;
-  if (ph.total > cap || (!out && ph.total)) return CUCM_ENOSPC;
-  ModelSource ms;
-  std::vector<uint8_t> image;
-  std::vector<uint8_t> pre(ph.prelearn);
-  if (ph.prelearn) {
-    HostModel hm;
-    if (ph.coded)
-      hm.prelearn_decode(h + kHeaderBytes, ph.pl_len, pre.data(), ph.prelearn);
-    else {
-      std::memcpy(pre.data(), h + kHeaderBytes, ph.prelearn);
-      hm.prelearn_train(pre.data(), ph.prelearn);
+  std::vector<std::vector<uint8_t>> host_copy(dev ? count : 0);
+  std::vector<const uint8_t *> h(count);
+  std::vector<Parsed> ph(count);
+  std::vector<std::vector<uint64_t>> off(count), len(count);
+  std::vector<uint32_t> ok;
+  for (uint32_t i = 0; i < count; i++) {
+    out_ns[i] = 0;
+    status[i] = ins[i] ? CUCM_OK : CUCM_EINVAL;
+    if (status[i]) continue;
+    h[i] = ins[i];
+    if (dev) {
+      host_copy[i].resize(ns[i]);
+      CK(cudaMemcpy(host_copy[i].data(), ins[i], ns[i], cudaMemcpyDeviceToHost));
+      h[i] = host_copy[i].data();
     }
-    hm.to_device(image, ms.init);
-    ms.image = &image;
-  } else {
-    zero_model(ms.init);
+    status[i] = parse_header(h[i], ns[i], ph[i]);
+    if (status[i]) continue;
+    out_ns[i] = ph[i].total;
+    if (ph[i].total > caps[i] || (!outs[i] && ph[i].total)) {
+      status[i] = CUCM_ENOSPC;
+      continue;
+    }
+    const uint64_t body_off = kHeaderBytes + ph[i].pl_len;
+    const uint64_t out_body = ph[i].total - ph[i].prelearn;
+    const uint64_t nchunks = (out_body + ph[i].cs - 1) / ph[i].cs;
+    status[i] = parse_batches(h[i] + body_off, ns[i] - body_off, nchunks, ph[i].batch, true, off[i], len[i]);
+    if (!status[i]) ok.push_back(i);
   }
-  const uint64_t body_off = kHeaderBytes + ph.pl_len;
-  const uint64_t body_n = n - body_off;
-  const uint64_t out_body = ph.total - ph.prelearn;
-  const uint64_t nchunks = (out_body + ph.cs - 1) / ph.cs;
-  std::vector<uint64_t> off, len;
-  rc = parse_batches(h + body_off, body_n, nchunks, ph.batch, true, off, len);
-  if (rc) return rc;
+  // groups: one per unit length for model-free containers, one per prelearned container
+  std::vector<std::vector<uint32_t>> groups;
+  for (uint32_t i : ok) {
+    if (ph[i].prelearn) {
+      groups.push_back({i});
+      continue;
+    }
+    bool placed = false;
+    for (auto &grp : groups)
+      if (!ph[grp[0]].prelearn && ph[grp[0]].unit == ph[i].unit) {
+        grp.push_back(i);
+        placed = true;
+        break;
+      }
+    if (!placed) groups.push_back({i});
+  }
   timing_begin(c);
-  const uint8_t *d_body;
-  uint8_t *d_o;
-  if (dev) {
-    d_body = in + body_off;
-    d_o = out + ph.prelearn;
-    if (ph.prelearn) CK(cudaMemcpyAsync(out, pre.data(), ph.prelearn, cudaMemcpyHostToDevice, c->stream));
-  } else {
-    CK(c->d_body.ensure(body_n ? body_n : 1));
-    if (body_n) CK(cudaMemcpyAsync(c->d_body.p, in + body_off, body_n, cudaMemcpyHostToDevice, c->stream));
-    d_body = c->d_body.as<uint8_t>();
-    CK(c->d_out.ensure(out_body ? out_body : 1));
-    d_o = c->d_out.as<uint8_t>();
-  }
-  rc = decode_chunks(c, d_body, off, len, out_body, ph.cs, ph.unit, ms, d_o);
-  if (rc) {
-    timing_end(c);
-    return rc;
-  }
-  if (!dev) {
-    if (ph.prelearn) std::memcpy(out, pre.data(), ph.prelearn);
-    if (out_body) CK(cudaMemcpyAsync(out + ph.prelearn, d_o, out_body, cudaMemcpyDeviceToHost, c->stream));
+  int rc = CUCM_OK;
+  for (const std::vector<uint32_t> &grp : groups) {
+    ModelSource ms;
+    std::vector<uint8_t> image, pre;
+    const uint32_t i0 = grp[0];
+    if (ph[i0].prelearn) {
+      HostModel hm;
+      pre.resize(ph[i0].prelearn);
+      if (ph[i0].coded)
+        hm.prelearn_decode(h[i0] + kHeaderBytes, ph[i0].pl_len, pre.data(), ph[i0].prelearn);
+      else {
+        std::memcpy(pre.data(), h[i0] + kHeaderBytes, ph[i0].prelearn);
+        hm.prelearn_train(pre.data(), ph[i0].prelearn);
+      }
+      hm.to_device(image, ms.init);
+      ms.image = &image;
+    } else {
+      zero_model(ms.init);
+    }
+    std::vector<uint64_t> bat(grp.size()), oat(grp.size());
+    uint64_t btot = 0, otot = 0;
+    for (size_t j = 0; j < grp.size(); j++) {
+      const uint32_t i = grp[j];
+      bat[j] = btot;
+      oat[j] = otot;
+      btot += ((ns[i] - kHeaderBytes - ph[i].pl_len) + 15) & ~15ull;
+      otot += ((ph[i].total - ph[i].prelearn) + 15) & ~15ull;
+    }
+    if (!dev) {
+      CK(c->d_body.ensure(btot ? btot : 1));
+      CK(c->d_out.ensure(otot ? otot : 1));
+    }
+    std::vector<DecJob> jobs(grp.size());
+    for (size_t j = 0; j < grp.size(); j++) {
+      const uint32_t i = grp[j];
+      const uint64_t body_off = kHeaderBytes + ph[i].pl_len;
+      const uint64_t body_n = ns[i] - body_off;
+      DecJob &jb = jobs[j];
+      if (dev) {
+        jb.d_body = ins[i] + body_off;
+        jb.d_out = outs[i] + ph[i].prelearn;
+        if (ph[i].prelearn) CK(cudaMemcpyAsync(outs[i], pre.data(), ph[i].prelearn, cudaMemcpyHostToDevice, c->stream));
+      } else {
+        if (body_n)
+          CK(cudaMemcpyAsync(c->d_body.as<uint8_t>() + bat[j], ins[i] + body_off, body_n, cudaMemcpyHostToDevice,
+                             c->stream));
+        jb.d_body = c->d_body.as<uint8_t>() + bat[j];
+        jb.d_out = c->d_out.as<uint8_t>() + oat[j];
+      }
+      jb.off = off[i];
+      jb.len = len[i];
+      jb.total = ph[i].total - ph[i].prelearn;
+      jb.cs = ph[i].cs;
+    }
+    rc = decode_jobs(c, jobs, ph[i0].unit, ms, c->d_body.cap + c->d_out.cap);
+    if (rc) {
+      for (uint32_t i : grp) status[i] = rc;
+      if (rc == CUCM_EFORMAT) {
+        rc = CUCM_OK;
+        continue;
+      }
+      break;
+    }
+    if (!dev) {
+      for (size_t j = 0; j < grp.size(); j++) {
+        const uint32_t i = grp[j];
+        if (ph[i].prelearn) std::memcpy(outs[i], pre.data(), ph[i].prelearn);
+        const uint64_t ob = ph[i].total - ph[i].prelearn;
+        if (ob)
+          CK(cudaMemcpyAsync(outs[i] + ph[i].prelearn, jobs[j].d_out, ob, cudaMemcpyDeviceToHost, c->stream));
+      }
+    }
+    CK(cudaStreamSynchronize(c->stream));
   }
   timing_end(c);
   CK(cudaStreamSynchronize(c->stream));
-  *out_n = ph.total;
+  if (rc) {
+    for (uint32_t i : ok)
+      if (!status[i]) status[i] = rc;
+    return rc;
+  }
+  for (uint32_t i = 0; i < count; i++)
+    if (status[i]) return status[i];
   return CUCM_OK;
 }
 
 int cucm_decompress(cucm_ctx *c, const uint8_t *in, uint64_t n, uint8_t *out, uint64_t cap, uint64_t *out_n) {
-  return decompress_impl(c, in, n, out, cap, out_n, false);
+  if (!c || !in || !out_n) return CUCM_EINVAL;
+  int st = 0;
+  return decompress_containers(c, 1, &in, &n, &out, &cap, out_n, &st, false);
 }
 
 int cucm_decompress_dev(cucm_ctx *c, const uint8_t *in, uint64_t n, uint8_t *out, uint64_t cap, uint64_t *out_n) {
-  return decompress_impl(c, in, n, out, cap, out_n, true);
+  if (!c || !in || !out_n) return CUCM_EINVAL;
+  int st = 0;
+  return decompress_containers(c, 1, &in, &n, &out, &cap, out_n, &st, true);
 }
 
 int cucm_compress_batch(cucm_ctx *c, const uint8_t *in, uint64_t n, uint64_t chunksize, uint32_t unit, uint8_t *out,
@@ -882,23 +795,21 @@ int cucm_compress_batch(cucm_ctx *c, const uint8_t *in, uint64_t n, uint64_t chu
   timing_begin(c);
   CK(c->d_body.ensure(n ? n : 1));
   if (n) CK(cudaMemcpyAsync(c->d_body.p, in, n, cudaMemcpyHostToDevice, c->stream));
-  CK(c->d_out.ensure(n * 2 + nchunks * (8 + 4096) + 64));
-  uint64_t body_n = 0;
-  rc = encode_and_pack(c, c->d_body.as<uint8_t>(), n, chunksize, unit, 0xffff, ms, false, c->d_out.as<uint8_t>(),
-                       c->d_out.cap, &body_n, nullptr);
-  if (rc) {
-    timing_end(c);
-    return rc;
+  Encoded e;
+  rc = encode_chunks(c, {Seg{c->d_body.as<uint8_t>(), n}}, chunksize, unit, ms, c->d_body.cap + c->d_out.cap, e);
+  const uint64_t body_n = rc ? 0 : layout_body(e, 0, 0xffff, false, nullptr, nullptr);
+  *out_n = body_n;
+  if (!rc && body_n > cap) rc = CUCM_ENOSPC;
+  if (!rc && body_n) {
+    CK(c->d_out.ensure(body_n));
+    std::vector<PackEntry> pe;
+    layout_body(e, 0, 0xffff, false, c->d_out.as<uint8_t>(), &pe);
+    rc = pack_bodies(c, pe);
+    if (!rc) CK(cudaMemcpyAsync(out, c->d_out.p, body_n, cudaMemcpyDeviceToHost, c->stream));
   }
-  if (body_n > cap) {
-    timing_end(c);
-    return CUCM_ENOSPC;
-  }
-  if (body_n) CK(cudaMemcpyAsync(out, c->d_out.p, body_n, cudaMemcpyDeviceToHost, c->stream));
   timing_end(c);
   CK(cudaStreamSynchronize(c->stream));
-  *out_n = body_n;
-  return CUCM_OK;
+  return rc;
 }
 
 int cucm_decompress_batch(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uint64_t chunksize, uint32_t unit,
@@ -906,8 +817,8 @@ int cucm_decompress_batch(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uin
   if (!c || !body || (!out && out_n)) return CUCM_EINVAL;
   if (chunksize == 0 || unit < 32 || unit > (uint32_t)kMaxUnit || unit % 32) return CUCM_EINVAL;
   uint64_t nchunks = (out_n + chunksize - 1) / chunksize;
-  std::vector<uint64_t> off, len;
-  int rc = parse_batches(body, body_n, nchunks, (uint32_t)std::max<uint64_t>(nchunks, 1), false, off, len);
+  DecJob jb;
+  int rc = parse_batches(body, body_n, nchunks, (uint32_t)std::max<uint64_t>(nchunks, 1), false, jb.off, jb.len);
   if (rc) return rc;
   std::lock_guard<std::mutex> g(c->mu);
   CK(cudaSetDevice(c->device));
@@ -917,38 +828,46 @@ int cucm_decompress_batch(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uin
   CK(c->d_body.ensure(body_n ? body_n : 1));
   CK(cudaMemcpyAsync(c->d_body.p, body, body_n, cudaMemcpyHostToDevice, c->stream));
   CK(c->d_out.ensure(out_n ? out_n : 1));
-  rc = decode_chunks(c, c->d_body.as<uint8_t>(), off, len, out_n, chunksize, unit, ms, c->d_out.as<uint8_t>());
-  if (rc) {
-    timing_end(c);
-    return rc;
-  }
-  if (out_n) CK(cudaMemcpyAsync(out, c->d_out.p, out_n, cudaMemcpyDeviceToHost, c->stream));
+  jb.d_body = c->d_body.as<uint8_t>();
+  jb.d_out = c->d_out.as<uint8_t>();
+  jb.total = out_n;
+  jb.cs = chunksize;
+  rc = decode_jobs(c, {jb}, unit, ms, c->d_body.cap + c->d_out.cap);
+  if (!rc && out_n) CK(cudaMemcpyAsync(out, c->d_out.p, out_n, cudaMemcpyDeviceToHost, c->stream));
   timing_end(c);
   CK(cudaStreamSynchronize(c->stream));
-  return CUCM_OK;
+  return rc;
+}
+
+static bool many_args_ok(cucm_ctx *c, uint32_t count, const void *ins, const uint64_t *ns, const void *outs,
+                         const uint64_t *caps, const uint64_t *out_ns, const int *status) {
+  return c && (count == 0 || (ins && ns && outs && caps && out_ns && status));
 }
 
 int cucm_compress_many(cucm_ctx *c, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
                        const cucm_params *p, uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns,
                        int *status) {
-  if (!c || (count && (!ins || !ns || !outs || !caps || !out_ns || !status))) return CUCM_EINVAL;
-  int first = CUCM_OK;
-  for (uint32_t i = 0; i < count; i++) {
-    status[i] = cucm_compress(c, ins[i], ns[i], p, outs[i], caps[i], &out_ns[i]);
-    if (status[i] && !first) first = status[i];
-  }
-  return first;
+  if (!many_args_ok(c, count, ins, ns, outs, caps, out_ns, status) || !p) return CUCM_EINVAL;
+  return compress_containers(c, count, ins, ns, p, outs, caps, out_ns, status, false);
+}
+
+int cucm_compress_many_dev(cucm_ctx *c, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                           const cucm_params *p, uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns,
+                           int *status) {
+  if (!many_args_ok(c, count, ins, ns, outs, caps, out_ns, status) || !p) return CUCM_EINVAL;
+  return compress_containers(c, count, ins, ns, p, outs, caps, out_ns, status, true);
 }
 
 int cucm_decompress_many(cucm_ctx *c, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
                          uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns, int *status) {
-  if (!c || (count && (!ins || !ns || !outs || !caps || !out_ns || !status))) return CUCM_EINVAL;
-  int first = CUCM_OK;
-  for (uint32_t i = 0; i < count; i++) {
-    status[i] = cucm_decompress(c, ins[i], ns[i], outs[i], caps[i], &out_ns[i]);
-    if (status[i] && !first) first = status[i];
-  }
-  return first;
+  if (!many_args_ok(c, count, ins, ns, outs, caps, out_ns, status)) return CUCM_EINVAL;
+  return decompress_containers(c, count, ins, ns, outs, caps, out_ns, status, false);
+}
+
+int cucm_decompress_many_dev(cucm_ctx *c, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                             uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns, int *status) {
+  if (!many_args_ok(c, count, ins, ns, outs, caps, out_ns, status)) return CUCM_EINVAL;
+  return decompress_containers(c, count, ins, ns, outs, caps, out_ns, status, true);
 }
 
 int cucm_last_device_ms(cucm_ctx *c, double *ms) {

@@ -79,8 +79,7 @@ def random_bytes(n, seed):
 
 def runs(n, seed):
     rng = np.random.default_rng(seed)
-    out = np.empty(0, dtype=np.uint8)
-    parts = []
+    parts = [np.empty(0, dtype=np.uint8)]
     total = 0
     while total < n:
         k = max(16, (n - total) // 150 + 16)

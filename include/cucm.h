@@ -111,14 +111,28 @@ int cucm_compress_batch(cucm_ctx *ctx, const uint8_t *in, uint64_t n, uint64_t c
 int cucm_decompress_batch(cucm_ctx *ctx, const uint8_t *body, uint64_t body_n, uint64_t chunksize, uint32_t unit,
                           uint8_t *out, uint64_t out_n);
 
-/* Many independent containers in one call (one persistent launch over all
- * their chunks).  Entry i reads ins[i][0..ns[i]) and writes outs[i] (caps[i]
- * bytes), its size to out_ns[i] and its status to status[i]. */
+/* Many independent containers in one call: the batched form.  Entry i
+ * reads ins[i][0..ns[i]) and writes outs[i] (caps[i] bytes), its size to
+ * out_ns[i] (the size it needs when status[i] is CUCM_ENOSPC) and its status
+ * to status[i]; the return value is the first failing status or CUCM_OK.
+ * Each container is byte-identical to what cucm_compress makes of it alone.
+ * Every chunk of every container without a prelearn prefix goes into ONE
+ * persistent launch (device work queue, longest chunk first); a container
+ * with a prelearn prefix has its own initial model and gets a launch of its
+ * own.  Decompression batches the containers of each unit length the same
+ * way.  No counterpart in the reference, which codes one file per process;
+ * it replaces running compress_file / decompress once per buffer.  Host
+ * buffers here, device buffers in the _dev forms. */
 int cucm_compress_many(cucm_ctx *ctx, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
                        const cucm_params *p, uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns,
                        int *status);
 int cucm_decompress_many(cucm_ctx *ctx, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
                          uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns, int *status);
+int cucm_compress_many_dev(cucm_ctx *ctx, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                           const cucm_params *p, uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns,
+                           int *status);
+int cucm_decompress_many_dev(cucm_ctx *ctx, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
+                             uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns, int *status);
 
 /* Device timing of the last call on this context, milliseconds (CUDA
  * events around the device work only). */

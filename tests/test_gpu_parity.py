@@ -36,10 +36,15 @@ def test_golden_compress(gpu_ctx, entry, form):
     assert got == golden
 
 
+# decoders: the one-warp kernel (units <= 256), and the generic kernel at
+# three speculation depths
+DECODERS = [(0, 0), (1, 1), (1, 4), (1, 8)]
+
+
 @pytest.mark.parametrize("entry", MANIFEST, ids=lambda e: e["name"])
-@pytest.mark.parametrize("spec", [1, 4, 8])
-def test_golden_decompress(gpu_ctx, entry, spec):
-    gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT, spec_bits=spec)
+@pytest.mark.parametrize("kernel,spec", DECODERS, ids=["warp", "generic1", "generic4", "generic8"])
+def test_golden_decompress(gpu_ctx, entry, kernel, spec):
+    gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT, spec_bits=spec, kernel=kernel)
     with open(os.path.join(GOLDEN, entry["name"] + ".cucm"), "rb") as f:
         golden = f.read()
     assert gpu_ctx.decompress(golden) == make_input(entry)
@@ -67,14 +72,18 @@ def test_against_oracle(gpu_ctx, oracle_mod, kind, size, cs, unit, pre, batch, f
     got = gpu_ctx.compress(data, cs, unit, pre, batch)
     assert got == want
     assert gpu_ctx.decompress(want) == data
+    gpu_ctx.set_tuning(form=form, kernel=1)
+    assert gpu_ctx.decompress(want) == data
 
 
 def test_speculation_depth_never_changes_output(gpu_ctx, oracle_mod):
     data = W.text(120000, 11).tobytes()
     blob = oracle_mod.compress(data, 32768, 128, 0, 100)
     for spec in range(1, 9):
-        gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT, spec_bits=spec)
+        gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT, spec_bits=spec, kernel=1)
         assert gpu_ctx.decompress(blob) == data
+    gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT, kernel=0)
+    assert gpu_ctx.decompress(blob) == data
 
 
 def test_batch_helpers_match_container(gpu_ctx, oracle_mod):
