@@ -24,6 +24,8 @@ FORM_AUTO, FORM_PLAIN, FORM_PERSISTENT = 0, 1, 2
 
 CUCM_OK = 0
 EINVAL, ENOSPC, EFORMAT = -1, -2, -3
+PENDING = 1
+OP_COMPRESS, OP_DECOMPRESS = 0, 1
 _ERRORS = {
     -1: "EINVAL", -2: "ENOSPC", -3: "EFORMAT", -4: "ENOMEM", -5: "ECUDA",
     -6: "ENODEV", -7: "ETIMEOUT", -8: "EBUSY", -9: "ENOTFOUND",
@@ -45,6 +47,12 @@ class Params(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("device_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double),
                 ("launches", ctypes.c_uint64), ("chunks", ctypes.c_uint64)]
+
+
+class ServerInfo(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint64), ("budget", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("bytes_in", ctypes.c_uint64), ("bytes_out", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("inflight", ctypes.c_uint64)]
 
 
 class Tuning(ctypes.Structure):
@@ -89,6 +97,14 @@ SIGNATURES = [
     ("cucm_decompress_many_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
                                                 _u64p, ctypes.POINTER(ctypes.c_void_p), _u64p, _u64p,
                                                 ctypes.POINTER(ctypes.c_int)]),
+    ("cucm_server_create", ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(Tuning),
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    ("cucm_server_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("cucm_serve_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                         ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    ("cucm_serve_poll", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       _u64p, ctypes.POINTER(ctypes.c_double)]),
+    ("cucm_server_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerInfo)]),
     ("cucm_last_device_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("cucm_last_launches", ctypes.c_int, [ctypes.c_void_p, _u64p]),
     ("cucm_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
@@ -133,6 +149,13 @@ def many_cap(n, chunksize, prelearn=0):
     redo the rare container that needs more."""
     nchunks = (max(n - prelearn, 0) + chunksize - 1) // chunksize
     return 64 + prelearn * 8 + nchunks * (8 + 2 * chunksize + 4096)
+
+
+def _buf_w(arr):
+    """(pointer, capacity, keepalive) of a writable numpy uint8 array."""
+    import numpy as np
+    a = arr.view(np.uint8).reshape(-1)
+    return a.ctypes.data, a.size, a
 
 
 def _buf(data):
@@ -381,3 +404,87 @@ def decompress_file(in_path, out_path):
     with open(out_path, "wb") as f:
         f.write(data)
     return len(data)
+
+
+class Server:
+    """The serving loop (cucm_server_*): submit compress / decompress requests
+    from any thread, poll for their results.  Requests that arrive while
+    others run are admitted as chunk slots and memory free up, and share
+    launches that overlap on the device; every result equals the
+    single-call API's."""
+
+    def __init__(self, device=0, hbm_budget=0, max_slots=0, kernel=0):
+        self._h = ctypes.c_void_p()
+        t = Tuning(FORM_PERSISTENT, 0, max_slots, hbm_budget, kernel)
+        rc = lib().cucm_server_create(device, hbm_budget, ctypes.byref(t), ctypes.byref(self._h))
+        if rc:
+            raise CucmError(rc, "cucm_server_create")
+        self._live = {}
+
+    def submit_compress(self, data, chunksize=1 << 20, unit=128, prelearn=0, batch=100, out=None):
+        """Queue a compression; `out` (optional, e.g. pinned) receives the container."""
+        p = default_params(chunksize, unit, prelearn, batch)
+        ptr, n, keep = _buf(data)
+        if out is None:
+            out = ctypes.create_string_buffer(max(many_cap(n, chunksize, prelearn), 1))
+            optr, cap = ctypes.addressof(out), len(out)
+        else:
+            optr, cap, out = _buf_w(out)
+        rid = ctypes.c_uint64()
+        rc = lib().cucm_serve_submit(self._h, OP_COMPRESS, ptr, n, ctypes.byref(p), optr, cap, ctypes.byref(rid))
+        if rc:
+            raise CucmError(rc, "cucm_serve_submit")
+        self._live[rid.value] = (keep, out, optr)
+        return rid.value
+
+    def submit_decompress(self, blob, out=None):
+        """Queue a decompression; `out` (optional) receives the original bytes."""
+        ptr, n, keep = _buf(blob)
+        size = ctypes.c_uint64()
+        rc = lib().cucm_decompressed_size(ptr, n, ctypes.byref(size))
+        if rc:
+            raise CucmError(rc, "cucm_decompressed_size")
+        if out is None:
+            out = ctypes.create_string_buffer(max(size.value, 1))
+            optr, cap = ctypes.addressof(out), size.value
+        else:
+            optr, cap, out = _buf_w(out)
+        rid = ctypes.c_uint64()
+        rc = lib().cucm_serve_submit(self._h, OP_DECOMPRESS, ptr, n, None, optr, cap, ctypes.byref(rid))
+        if rc:
+            raise CucmError(rc, "cucm_serve_submit")
+        self._live[rid.value] = (keep, out, optr)
+        return rid.value
+
+    def poll(self, rid, timeout_ms=-1):
+        """None while pending, else (status, output bytes or None, latency ms)."""
+        st = ctypes.c_int()
+        n = ctypes.c_uint64()
+        lat = ctypes.c_double()
+        rc = lib().cucm_serve_poll(self._h, rid, int(timeout_ms), ctypes.byref(st), ctypes.byref(n),
+                                   ctypes.byref(lat))
+        if rc == PENDING:
+            return None
+        if rc:
+            raise CucmError(rc, "cucm_serve_poll")
+        keep, out, optr = self._live.pop(rid)
+        data = ctypes.string_at(optr, n.value) if st.value == 0 else None
+        return st.value, data, lat.value
+
+    def stats(self):
+        info = ServerInfo()
+        rc = lib().cucm_server_stats(self._h, ctypes.byref(info))
+        if rc:
+            raise CucmError(rc, "cucm_server_stats")
+        return {f: getattr(info, f) for f, _ in ServerInfo._fields_}
+
+    def close(self):
+        if self._h:
+            lib().cucm_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

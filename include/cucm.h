@@ -134,6 +134,46 @@ int cucm_compress_many_dev(cucm_ctx *ctx, uint32_t count, const uint8_t *const *
 int cucm_decompress_many_dev(cucm_ctx *ctx, uint32_t count, const uint8_t *const *ins, const uint64_t *ns,
                              uint8_t *const *outs, const uint64_t *caps, uint64_t *out_ns, int *status);
 
+/* Serving loop (continuous batching).  No counterpart in the reference.
+ * A server owns one device, a pool of chunk-slot tables and a buffer pool
+ * carved from `hbm_budget` bytes of device memory (0 = 90% of free memory),
+ * and a scheduler thread.  Requests are submitted from any thread and admitted
+ * in arrival order as slots and buffer memory free up; admitted requests of
+ * one kind (operation, unit length) share one persistent launch, and
+ * launches on their own streams overlap on the device.  Every result is
+ * byte-identical to cucm_compress / cucm_decompress of the same input.
+ * Buffers passed to submit (host memory; pinned memory lets the copies run
+ * asynchronously) must stay valid until poll reports the request done. */
+#define CUCM_PENDING 1  /* cucm_serve_poll: the request has not finished */
+typedef struct cucm_server cucm_server;
+typedef enum cucm_op { CUCM_OP_COMPRESS = 0, CUCM_OP_DECOMPRESS = 1 } cucm_op;
+typedef struct cucm_server_info {
+  uint64_t slots;      /* chunk slots in the pool */
+  uint64_t budget;     /* device bytes the server may hold */
+  uint64_t completed;  /* requests finished */
+  uint64_t bytes_in;   /* input bytes of finished requests */
+  uint64_t bytes_out;  /* output bytes of finished requests */
+  uint64_t launches;   /* engine launches so far */
+  uint64_t queued;     /* requests waiting for admission */
+  uint64_t inflight;   /* launches on the device */
+} cucm_server_info;
+int cucm_server_create(int device, uint64_t hbm_budget, const cucm_tuning *tuning, cucm_server **out);
+/* Finishes every submitted request, then releases the server. */
+int cucm_server_destroy(cucm_server *srv);
+/* op CUCM_OP_COMPRESS: `in`/`n` is the buffer, `p` the stream parameters,
+ * `out`/`cap` receives the container.  CUCM_OP_DECOMPRESS: `in`/`n` is a
+ * container, `p` is ignored, `out`/`cap` receives the original bytes.
+ * *id identifies the request; CUCM_EBUSY when the queue is full. */
+int cucm_serve_submit(cucm_server *srv, int op, const uint8_t *in, uint64_t n, const cucm_params *p, uint8_t *out,
+                      uint64_t cap, uint64_t *id);
+/* Waits up to timeout_ms (0 = just look, < 0 = until done) for request `id`.
+ * CUCM_OK when it is done: *status is its result (a CUCM_* code), *out_n its
+ * output size (the size needed when *status is CUCM_ENOSPC), *latency_ms the
+ * time from submit to completion; the id is then forgotten.  CUCM_PENDING
+ * when it is still queued or running, CUCM_ENOTFOUND for an unknown id. */
+int cucm_serve_poll(cucm_server *srv, uint64_t id, int timeout_ms, int *status, uint64_t *out_n, double *latency_ms);
+int cucm_server_stats(cucm_server *srv, cucm_server_info *info);
+
 /* Device timing of the last call on this context, milliseconds (CUDA
  * events around the device work only). */
 int cucm_last_device_ms(cucm_ctx *ctx, double *ms);

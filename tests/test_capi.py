@@ -43,6 +43,16 @@ def test_ctx_create_without_gpu_fails_loudly(cucm_lib):
     assert cucm_lib.cucm_ctx_create(0, None, ctypes.byref(h)) == -6  # CUCM_ENODEV
     with pytest.raises(cucm_b200.CucmError):
         cucm_b200.Context(0)
+    assert cucm_lib.cucm_server_create(0, 0, None, ctypes.byref(h)) == -6
+    with pytest.raises(cucm_b200.CucmError):
+        cucm_b200.Server(0)
+
+
+def test_serve_calls_reject_bad_arguments(cucm_lib):
+    rid = ctypes.c_uint64()
+    assert cucm_lib.cucm_serve_submit(None, 0, None, 0, None, None, 0, ctypes.byref(rid)) == -1
+    assert cucm_lib.cucm_serve_poll(None, 1, 0, None, None, None) == -1
+    assert cucm_lib.cucm_server_destroy(None) == -1
 
 
 def test_default_params_match_reference_cli(cucm_lib):
