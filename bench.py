@@ -11,6 +11,16 @@ alone.  The input (256 MiB, plus 48 GiB of chunk tables touched at random)
 is larger than L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload mixed256M|batch|serve|small]
+
+Other workloads (one JSON line each, not the headline):
+  batch  -- 4096 independent buffers, log-uniform 4 KiB..4 MiB, 256 KiB chunks:
+            the batched persistent form (one launch for all buffers) against
+            the plain form (one launch per chunk), byte-identical outputs;
+  serve  -- the serving loop under Poisson request streams at stated offered
+            loads: p50/p99 latency and sustained MB/s against serving the
+            same stream one request at a time;
+  small  -- 1 MiB of text at 64 KiB chunks, one round trip (profiling case).
 
 --impl reference times the reference's own implementation of the path on the
 host cores: its two programs built for the CPU from its unmodified sources
@@ -49,6 +59,11 @@ def parse():
     ap.add_argument("--form", default="persistent", choices=["persistent", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="mixed256M", choices=["mixed256M", "batch", "serve", "small"])
+    ap.add_argument("--plain-sample", type=int, default=512, help="buffers the plain form codes (batch)")
+    ap.add_argument("--requests", type=int, default=48, help="requests per offered load (serve)")
+    ap.add_argument("--loads", default="0.02,0.2,2,8,32", help="offered loads in GB/s (serve)")
+    ap.add_argument("--small-bytes", type=int, default=1 << 20, help="text bytes of the small workload")
     return ap.parse_args()
 
 
@@ -70,11 +85,12 @@ def measured_peak():
 
 
 def profile_traffic():
-    """DRAM bytes per compress launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "compress_kernel_mixed256M.json")
+    """DRAM bytes per full-size launch of each kernel, from the committed ncu
+    summary (profiles/traffic_mixed256M.json), if present."""
+    p = os.path.join(ROOT, "profiles", "traffic_mixed256M.json")
     try:
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            return {k: v.get("dram_bytes_per_launch") for k, v in json.load(f).items() if isinstance(v, dict)}
     except Exception:
         return None
 
@@ -244,6 +260,10 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    if args.workload != "mixed256M":
+        if rank == 0:
+            {"batch": run_batch, "serve": run_serve, "small": run_small}[args.workload](args)
+        return
     import numpy as np
     import torch
     import cucm_b200 as cc
@@ -347,14 +367,19 @@ def main():
         return
 
     peak, peak_kind = measured_peak()
-    kc_launch = kc / K
-    achieved = ALGO_BYTES_PER_BYTE * n / (kc_launch / 1e3) / 1e9 if kc_launch > 0 else None
     traffic = profile_traffic()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "peak_source": peak_kind, "kernel": "compress_fast_kernel",
-                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_BYTE * n,
-                "kernel_ms_per_launch": kc_launch}
+
+    def roof(kernel, ms_per_launch):
+        ach = ALGO_BYTES_PER_BYTE * n / (ms_per_launch / 1e3) / 1e9 if ms_per_launch > 0 else None
+        return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": (ach / peak) if ach else None, "traffic": traffic.get(kernel) if traffic else None,
+                "peak_source": peak_kind, "kernel": kernel, "algorithmic_bytes_per_launch": ALGO_BYTES_PER_BYTE * n,
+                "kernel_ms_per_launch": ms_per_launch}
+    r_comp = roof("compress_fast_kernel", kc / K)
+    r_dec = roof("decompress_warp_kernel", kd / K)
+    # the dominant kernel of the step (the longer one) carries the roofline
+    roofline = dict(r_dec if kd >= kc else r_comp)
+    roofline["other"] = r_comp if kd >= kc else r_dec
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -377,6 +402,198 @@ def main():
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# Other workloads
+
+def _mbps(nbytes, ms):
+    return nbytes / (ms / 1e3) / 1e6 if ms > 0 else None
+
+
+def run_small(args):
+    """1 MiB of text at 64 KiB chunks (16 chunks): one compress and one
+    decompress through the device API -- the case the ncu captures use."""
+    import torch
+    import cucm_b200 as cc
+    from cucm_b200 import workloads as W
+    data, p = W.config0()
+    data = data[:args.small_bytes]
+    n = data.size
+    ctx = cc.Context(0)
+    d_in = torch.from_numpy(data).cuda()
+    cap = cc.lib().cucm_compress_bound(n, cc.default_params(**p))
+    d_c = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    d_o = torch.empty(n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    m = ctx.compress_dev(d_in.data_ptr(), n, d_c.data_ptr(), cap, **p)
+    sc = ctx.last_stats()
+    ctx.decompress_dev(d_c.data_ptr(), m, d_o.data_ptr(), n)
+    sd = ctx.last_stats()
+    ok = bool(torch.equal(d_o, d_in))
+    print(json.dumps({"metric": "small round trip MB/s",
+                      "workload": "%d bytes of text, 64 KiB chunks (%d)" % (n, (n + 65535) // 65536),
+                      "compress_MBps": _mbps(n, sc["device_ms"]), "decompress_MBps": _mbps(n, sd["device_ms"]),
+                      "compressed_bytes": m, "byte_exact": ok}), flush=True)
+    if not ok:
+        raise SystemExit("round trip mismatch")
+
+
+def run_batch(args):
+    """Config 2 / 3: 4096 buffers, batched persistent form vs plain form."""
+    import numpy as np
+    import torch
+    import cucm_b200 as cc
+    from cucm_b200 import workloads as W
+    bufs, p = W.config2()
+    cs = p["chunksize"]
+    ctx = cc.Context(0)
+
+    def dev_round(sub, form):
+        ctx.set_tuning(form=form)
+        d_in = [torch.from_numpy(b).cuda() if len(b) else torch.zeros(1, dtype=torch.uint8, device="cuda")
+                for b in sub]
+        caps = [cc.many_cap(len(b), cs) for b in sub]
+        d_out = [torch.empty(c, dtype=torch.uint8, device="cuda") for c in caps]
+        back = [torch.empty(max(len(b), 1), dtype=torch.uint8, device="cuda") for b in sub]
+        torch.cuda.synchronize()
+        sizes, st = ctx.compress_many_dev([(x.data_ptr(), len(b)) for x, b in zip(d_in, sub)],
+                                          [(x.data_ptr(), c) for x, c in zip(d_out, caps)], **p)
+        sc = ctx.last_stats()
+        if any(st):
+            raise SystemExit("compress_many_dev failed: %s" % sorted(set(st)))
+        _, st2 = ctx.decompress_many_dev([(x.data_ptr(), m) for x, m in zip(d_out, sizes)],
+                                         [(x.data_ptr(), len(b)) for x, b in zip(back, sub)])
+        sd = ctx.last_stats()
+        if any(st2):
+            raise SystemExit("decompress_many_dev failed: %s" % sorted(set(st2)))
+        ok = all(torch.equal(x[:len(b)], y[:len(b)]) for x, y, b in zip(back, d_in, sub))
+        blobs = [bytes(x[:m].cpu().numpy().tobytes()) for x, m in zip(d_out, sizes)]
+        nb = sum(len(b) for b in sub)
+        return dict(bytes=nb, compressed=sum(sizes), compress_ms=sc["device_ms"], decompress_ms=sd["device_ms"],
+                    compress_launches=sc["launches"], decompress_launches=sd["launches"],
+                    compress_MBps=_mbps(nb, sc["device_ms"]), decompress_MBps=_mbps(nb, sd["device_ms"]),
+                    round_trip_MBps=_mbps(nb, sc["device_ms"] + sd["device_ms"]), roundtrip_ok=ok), blobs
+
+    for _ in range(max(args.warmup, 0)):
+        dev_round(bufs[:64], cc.FORM_PERSISTENT)
+    sub = bufs[:args.plain_sample]
+    plain, blobs_p = dev_round(sub, cc.FORM_PLAIN)
+    batched_sub, blobs_b = dev_round(sub, cc.FORM_PERSISTENT)
+    full, _ = dev_round(bufs, cc.FORM_PERSISTENT)
+    same = blobs_p == blobs_b
+    # end to end through the host-buffer batched API (pinned inputs)
+    pinned = [torch.from_numpy(b).pin_memory().numpy() if len(b) else b for b in bufs]
+    ctx.set_tuning(form=cc.FORM_PERSISTENT)
+    t0 = time.perf_counter()
+    blobs_h = ctx.compress_many(pinned, **p)
+    e_c = ctx.last_stats()["device_ms"]
+    back_h = ctx.decompress_many(blobs_h)
+    e_d = ctx.last_stats()["device_ms"]
+    wall = time.perf_counter() - t0
+    e2e_ok = all(x == y.tobytes() for x, y in zip(back_h, bufs))
+    nfull = full["bytes"]
+    line = {
+        "metric": "batched compress+decompress round-trip MB/s", "value": full["round_trip_MBps"], "unit": "MB/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "4096 buffers, log-uniform 4 KiB..4 MiB (%.2f GiB), 0.5 text / 0.25 walk / "
+                               "0.15 random / 0.1 runs, 256 KiB chunks, unit 128" % (nfull / 2**30),
+                   "form": "persistent (one launch for all buffers)"},
+        "batched": full,
+        "plain_sample": {"buffers": len(sub), "plain": plain, "batched": batched_sub,
+                         "speedup_compress": batched_sub["compress_MBps"] / plain["compress_MBps"],
+                         "speedup_decompress": batched_sub["decompress_MBps"] / plain["decompress_MBps"],
+                         "byte_identical": same},
+        "e2e": {"value": _mbps(nfull, e_c + e_d), "unit": "MB/s", "wall_s": wall, "roundtrip_ok": e2e_ok,
+                "h2d_bytes_per_step": nfull + full["compressed"], "d2h_bytes_per_step": nfull + full["compressed"]},
+        "byte_exact": bool(full["roundtrip_ok"] and plain["roundtrip_ok"] and same and e2e_ok),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _pctl(xs, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(xs), q)) if xs else None
+
+
+def run_serve(args):
+    """Config 4: the serving loop against one-request-at-a-time serving.  The
+    per-request form runs first on a context of its own, which is then
+    released, so that the server alone holds its HBM budget."""
+    import numpy as np
+    import torch
+    import cucm_b200 as cc
+    from cucm_b200 import workloads as W
+    loads = [float(x) for x in args.loads.split(",")]
+    ctx = cc.Context(0)
+    streams = []
+    for li, gbps in enumerate(loads):
+        arrivals, comp, bufs, p = W.config4(args.requests, gbps, seed=4 + li)
+        cs = p["chunksize"]
+        dec_idx = [i for i in range(len(bufs)) if not comp[i]]
+        blobs = ctx.compress_many([bufs[i] for i in dec_idx], **p) if dec_idx else []
+        inputs = []
+        for i, b in enumerate(bufs):
+            src = b if comp[i] else np.frombuffer(blobs[dec_idx.index(i)], dtype=np.uint8)
+            inputs.append(torch.from_numpy(src.copy()).pin_memory().numpy() if len(src) else src)
+        # one request at a time, in arrival order (the plain per-request form)
+        lat_p, res_p = [], []
+        t0 = time.perf_counter()
+        for i in range(len(bufs)):
+            d = t0 + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            out = ctx.compress(inputs[i], **p) if comp[i] else ctx.decompress(inputs[i])
+            lat_p.append((time.perf_counter() - t0 - arrivals[i]) * 1e3)
+            res_p.append(out)
+        t_plain = time.perf_counter() - t0
+        streams.append((gbps, arrivals, comp, bufs, p, inputs, lat_p, res_p, t_plain))
+    ctx.close()
+
+    srv = cc.Server(0, hbm_budget=120 * 10**9)
+    results = []
+    for gbps, arrivals, comp, bufs, p, inputs, lat_p, res_p, t_plain in streams:
+        cs = p["chunksize"]
+        caps = [cc.many_cap(len(b), cs) if comp[i] else max(len(b), 1) for i, b in enumerate(bufs)]
+        outs = [torch.empty(c, dtype=torch.uint8).pin_memory().numpy() for c in caps]
+        nbytes = sum(len(b) for b in bufs)
+        lat, res = [None] * len(bufs), [None] * len(bufs)
+        t0 = time.perf_counter()
+        ids = []
+        for i in range(len(bufs)):
+            d = t0 + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            if comp[i]:
+                ids.append(srv.submit_compress(inputs[i], out=outs[i], **p))
+            else:
+                ids.append(srv.submit_decompress(inputs[i], out=outs[i]))
+        for i, rid in enumerate(ids):
+            st, data, ms = srv.poll(rid, -1)
+            if st:
+                raise SystemExit("serve request %d failed: %d" % (i, st))
+            lat[i], res[i] = ms, data
+        t_srv = time.perf_counter() - t0
+        exact = all(a == b for a, b in zip(res, res_p)) and all(
+            res[i] == bufs[i].tobytes() for i in range(len(bufs)) if not comp[i])
+        results.append({"offered_GBps": gbps, "requests": len(bufs), "bytes": nbytes,
+                        "serve": {"p50_ms": _pctl(lat, 50), "p99_ms": _pctl(lat, 99),
+                                  "sustained_MBps": nbytes / t_srv / 1e6},
+                        "one_at_a_time": {"p50_ms": _pctl(lat_p, 50), "p99_ms": _pctl(lat_p, 99),
+                                          "sustained_MBps": nbytes / t_plain / 1e6},
+                        "byte_exact": bool(exact)})
+    info = srv.stats()
+    srv.close()
+    best = max(r["serve"]["sustained_MBps"] for r in results)
+    print(json.dumps({"metric": "serving sustained MB/s and p50/p99 latency", "value": best, "unit": "MB/s",
+                      "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+                      "config": {"workload": "Poisson request streams, %d requests per load, sizes log-uniform "
+                                             "1 KiB..16 MiB, 70%% compress / 30%% decompress, content as the "
+                                             "4096-buffer set, 256 KiB chunks, HBM budget 120 GB"
+                                             % args.requests,
+                                 "slots": info["slots"]},
+                      "levels": results,
+                      "byte_exact": all(r["byte_exact"] for r in results)}), flush=True)
 
 
 if __name__ == "__main__":

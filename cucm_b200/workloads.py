@@ -15,7 +15,9 @@ which is available here; these generators stand in for them:
 Config builders follow the workload descriptions the benchmark uses:
 config0 (1 MiB text, 64 KiB chunks), config1 (256 MiB mixed, 1 MiB chunks,
 64 KiB blocks in seeded order), config2 (4096 buffers, log-uniform sizes in
-[4 KiB, 4 MiB], one content type each, 256 KiB chunks).
+[4 KiB, 4 MiB], one content type each, 256 KiB chunks) and config4 (a
+serving request stream: Poisson arrivals, sizes log-uniform in [1 KiB,
+16 MiB], 70% compress / 30% decompress, content drawn as in config2).
 """
 import ctypes
 import functools
@@ -141,3 +143,20 @@ def config2(count=4096, lo=4096, hi=4 << 20, seed=2):
     sizes, kinds = config2_sizes(count, lo, hi, seed)
     bufs = [make(KINDS[k], int(s), _derive(seed, 1000 + i)) for i, (s, k) in enumerate(zip(sizes, kinds))]
     return bufs, dict(chunksize=256 << 10, unit=128, prelearn=0, batch=100)
+
+
+def config4(count, offered_gbps, lo=1024, hi=16 << 20, seed=4):
+    """A serving request stream of `count` requests at an offered load of
+    `offered_gbps` GB/s: Poisson arrivals (exponential gaps whose mean is the
+    mean request size over the load), sizes log-uniform in [lo, hi], 70%
+    compress / 30% decompress, content drawn as in config2; 256 KiB chunks.
+    Returns (arrival seconds, is_compress flags, buffers, params)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), size=count))).astype(np.int64)
+    kinds = rng.choice(4, size=count, p=[0.5, 0.25, 0.15, 0.10])
+    comp = rng.random(count) < 0.7
+    mean = (hi - lo) / np.log(hi / lo)
+    gaps = rng.exponential(mean / (offered_gbps * 1e9), size=count)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    bufs = [make(KINDS[k], int(s), _derive(seed, 5000 + i)) for i, (s, k) in enumerate(zip(sizes, kinds))]
+    return arrivals, comp, bufs, dict(chunksize=256 << 10, unit=128, prelearn=0, batch=100)
