@@ -63,7 +63,10 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=512, help="buffers the plain form codes (batch)")
     ap.add_argument("--requests", type=int, default=48, help="requests per offered load (serve)")
     ap.add_argument("--loads", default="0.02,0.2,2,8,32", help="offered loads in GB/s (serve)")
-    ap.add_argument("--small-bytes", type=int, default=1 << 20, help="text bytes of the small workload")
+    ap.add_argument("--small-bytes", type=int, default=1 << 20, help="bytes of the small workload")
+    ap.add_argument("--small-source", default="text", choices=["text", "mixed"],
+                    help="small workload content: text, or the head of the 256 MiB mixed buffer")
+    ap.add_argument("--small-chunk", type=int, default=64 << 10, help="chunk size of the small workload")
     return ap.parse_args()
 
 
@@ -376,7 +379,7 @@ def main():
                 "peak_source": peak_kind, "kernel": kernel, "algorithmic_bytes_per_launch": ALGO_BYTES_PER_BYTE * n,
                 "kernel_ms_per_launch": ms_per_launch}
     r_comp = roof("compress_fast_kernel", kc / K)
-    r_dec = roof("decompress_warp_kernel", kd / K)
+    r_dec = roof("decompress_pair_kernel", kd / K)
     # the dominant kernel of the step (the longer one) carries the roofline
     roofline = dict(r_dec if kd >= kc else r_comp)
     roofline["other"] = r_comp if kd >= kc else r_dec
@@ -412,13 +415,18 @@ def _mbps(nbytes, ms):
 
 
 def run_small(args):
-    """1 MiB of text at 64 KiB chunks (16 chunks): one compress and one
-    decompress through the device API -- the case the ncu captures use."""
+    """A small case of the same path -- by default 1 MiB of text at 64 KiB
+    chunks, or the head of the 256 MiB mixed buffer -- one compress and one
+    decompress through the device API: the case the ncu captures use."""
     import torch
     import cucm_b200 as cc
     from cucm_b200 import workloads as W
-    data, p = W.config0()
-    data = data[:args.small_bytes]
+    if args.small_source == "text":
+        data, _ = W.config0()
+    else:
+        data, _ = W.config1()
+    data = data[:args.small_bytes].copy()
+    p = dict(PARAMS, chunksize=args.small_chunk)
     n = data.size
     ctx = cc.Context(0)
     d_in = torch.from_numpy(data).cuda()
@@ -432,8 +440,10 @@ def run_small(args):
     sd = ctx.last_stats()
     ok = bool(torch.equal(d_o, d_in))
     print(json.dumps({"metric": "small round trip MB/s",
-                      "workload": "%d bytes of text, 64 KiB chunks (%d)" % (n, (n + 65535) // 65536),
+                      "workload": "%d bytes of %s, %d-byte chunks (%d)" % (n, args.small_source, p["chunksize"],
+                                                                         (n + p["chunksize"] - 1) // p["chunksize"]),
                       "compress_MBps": _mbps(n, sc["device_ms"]), "decompress_MBps": _mbps(n, sd["device_ms"]),
+                      "kernel_ms": {"compress": sc["kernel_ms"], "decompress": sd["kernel_ms"]},
                       "compressed_bytes": m, "byte_exact": ok}), flush=True)
     if not ok:
         raise SystemExit("round trip mismatch")

@@ -392,6 +392,7 @@ int decode_jobs(cucm_ctx *c, const std::vector<DecJob> &jobs, uint32_t unit, con
   CK(cudaMemcpyAsync(&status, c->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (status & kDevBadTask) return CUCM_EFORMAT;
+  if (status & kDevTimeout) return CUCM_ETIMEOUT;
   return CUCM_OK;
 }
 

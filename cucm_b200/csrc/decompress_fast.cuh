@@ -1,49 +1,53 @@
-// decompress_fast.cuh -- chunk decoder, one warp per chunk, units of 32..256 bits.
+// decompress_fast.cuh -- chunk decoder, two warps per chunk, units of 32..256 bits.
 //
 // Included by engine_kernels.cu (shares its tables and helpers).
 //
 // The reference decodes a unit in speculation steps of L+1 bits, each step
 // three launches and a host round trip (cucm_decompress_v2.cu:977-1032).
-// Here one warp owns a chunk and decodes it a nibble ("round") at a time:
+// Here a pair of warps owns a chunk and decodes it a nibble ("round") at a
+// time.
 //
-//   * the 15 nodes of the nibble's speculation tree (every prefix of 0..3
-//     bits) get their 8 context keys and frozen slot states -- one lane per
-//     node, 8 gathers in flight per lane, so a round costs one memory
-//     round trip;
-//   * while those gathers are in flight the same warp runs the model update
-//     of the previous round's 4 bits (lane = order): the bit-history walk
-//     through a per-unit overlay (slot -> live state), the StateMap
-//     probability chain and the mixer deltas, all in bit order;
-//   * each node lane stretches, mixes and squashes its prediction against
-//     the frozen model, and the warp decodes the 4 bits uniformly (every lane
-//     runs the same coder arithmetic; the split point of a node comes from
-//     its lane by shuffle);
-//   * the 4 lanes on the decoded path record keys, states and inputs of their
-//     bit for the next round's update.
+// The decoding warp:
+//   * gives the 15 nodes of the nibble's speculation tree (every prefix of
+//     0..3 bits) their 8 context keys and frozen slot states -- one lane per
+//     node, 8 gathers in flight per lane, so a round costs one memory round
+//     trip;
+//   * stretches, mixes and squashes each node's prediction against the
+//     frozen model and decodes the 4 bits uniformly (every lane runs the same
+//     coder arithmetic; the split point of a node comes from its lane by
+//     shuffle);
+//   * has the 4 lanes on the decoded path record keys, states and mixer
+//     inputs of their bit in a per-unit ring, and publishes the round.
+// The updating warp follows one round behind (lane = order): the bit-history
+// walk through a per-unit overlay (slot -> live state), the StateMap
+// probability chain and the mixer deltas, all in bit order.  Nothing the
+// decoding warp reads changes before the unit ends, so the two only meet
+// there: the overlay's states go to the slot tables, the live probabilities
+// become the frozen ones and the summed mixer deltas join the weights
+// (updateStateMap / updateMixer, cucm_decompress_v2.cu:870-896).  Rounds
+// never straddle a unit or byte boundary: units are multiples of 32 bits.
 //
-// At a unit end the overlay's states are written to the slot tables, the
-// live probabilities become the frozen ones and the summed mixer deltas are
-// added to the weights (updateStateMap / updateMixer,
-// cucm_decompress_v2.cu:870-896).  Rounds never straddle a unit or byte
-// boundary: units are multiples of 32 bits.
-//
-// Several warps of a CTA decode independent chunks and share the read-only
-// tables.
+// Several warp pairs of a CTA decode independent chunks and share the
+// read-only tables.
 
 constexpr int kDecMaxUnit = 256;
-constexpr int kDecMaxWarps = 8;
-constexpr int kDecWin = 2048;   // payload window per warp (bytes)
-constexpr int kDecNodes = 15;   // nodes of a 4-bit speculation tree
+constexpr int kDecMaxPairs = 8;          // chunks per CTA
+constexpr int kDecWin = 2048;            // payload window per chunk (bytes)
+constexpr int kDecNodes = 15;            // nodes of a 4-bit speculation tree
+constexpr int kDecRecBytes = 240;        // one round's records
+constexpr uint32_t kDecSpinLimit = 1u << 26;  // bound of the updater's wait for a round
 
 struct DecLayout {
-  int U, NS, logNS, warps;
-  size_t off_spf, off_spl, off_w, off_dw, off_ovk, off_ovs, off_ovl, off_ovn, off_rk, off_rs, off_rsmp, off_rpc,
-      off_win, off_outb, per_warp, off_tab, total;
+  int U, NS, logNS, warps, rounds;
+  size_t off_spf, off_spl, off_w, off_dw, off_ovk, off_ovs, off_ovl, off_ovn, off_prog, off_rk, off_rs, off_rsmp,
+      off_rpc, off_win, off_outb, per_warp, off_tab, total;
 };
 
+// Shared memory of `warps` chunks (warp pairs) and the shared tables.
 __host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
   DecLayout L;
   L.U = U;
+  L.rounds = U / 4;
   L.NS = next_pow2(2 * U);  // overlay slots per order (load <= 1/2)
   L.logNS = ilog2(L.NS);
   L.warps = warps;
@@ -61,10 +65,11 @@ __host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
   L.off_ovs = take((size_t)kOrders * L.NS);                    // overlay live states
   L.off_ovl = take(sizeof(uint16_t) * U * kOrders);            // overlay entries in use [entry][order]
   L.off_ovn = take(sizeof(int) * kOrders);
-  L.off_rk = take(sizeof(uint32_t) * 2 * 4 * kOrders);         // records [round parity][bit][order]
-  L.off_rs = take((size_t)2 * 4 * kOrders);
-  L.off_rsmp = take(sizeof(int16_t) * 2 * 4 * kOrders);
-  L.off_rpc = take(sizeof(uint32_t) * 2 * 4);                  // pr | cxt << 16 | y << 24
+  L.off_prog = take(sizeof(uint32_t) * 4);                     // rounds published; task index
+  L.off_rk = take(sizeof(uint32_t) * L.rounds * 4 * kOrders);  // records [round][bit][order]
+  L.off_rs = take((size_t)L.rounds * 4 * kOrders);
+  L.off_rsmp = take(sizeof(int16_t) * L.rounds * 4 * kOrders);
+  L.off_rpc = take(sizeof(uint32_t) * L.rounds * 4);           // pr | cxt << 16 | y << 24
   L.off_win = take((size_t)kDecWin);
   L.off_outb = take((size_t)kDecMaxUnit / 8);
   L.per_warp = o;
@@ -80,6 +85,7 @@ struct DecSmem {
   uint8_t *ovs;
   uint16_t *ovl;
   int *ovn;
+  volatile uint32_t *prog;
   uint32_t *rk;
   uint8_t *rs;
   int16_t *rsmp;
@@ -98,6 +104,7 @@ __device__ inline DecSmem carve_dec(uint8_t *base, const DecLayout &L, int warp)
   s.ovs = b + L.off_ovs;
   s.ovl = reinterpret_cast<uint16_t *>(b + L.off_ovl);
   s.ovn = reinterpret_cast<int *>(b + L.off_ovn);
+  s.prog = reinterpret_cast<volatile uint32_t *>(b + L.off_prog);
   s.rk = reinterpret_cast<uint32_t *>(b + L.off_rk);
   s.rs = b + L.off_rs;
   s.rsmp = reinterpret_cast<int16_t *>(b + L.off_rsmp);
@@ -127,107 +134,217 @@ __device__ inline long long dec_refill(uint8_t *win, const uint8_t *pay, uint64_
 // bit order: the live state of each slot (overlay, else the frozen state the
 // prediction saw), its next state, the StateMap probability of the live state
 // (cucm_decompress_v2.cu:870-883) and the mixer deltas (:885-896).
+//
+// All shared-memory reads of the four bits are issued before any write:
+// what an earlier bit of the round changes for a later one -- the same
+// slot's state, the same state's probability, an overlay entry it claims --
+// is carried forward in registers, and the writes follow in bit order, so a
+// later write to the same place wins as it would one bit at a time.
+// `nov` is this lane's count of overlay entries in use (its order's list).
 __device__ __forceinline__ void dec_update_round(const DecSmem &s, const Tables *tab, const DecLayout &L, int o,
-                                                 int buf) {
+                                                 int rd, int &nov) {
   uint32_t *ovk = s.ovk + o * L.NS;
   uint8_t *ovs = s.ovs + o * L.NS;
+  const uint32_t mask = (uint32_t)(L.NS - 1);
+  uint32_t k[4], b[4], e[4];
+  int fz[4], sm[4], y[4], os[4];
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) {
-    const int r = (buf * 4 + i) * kOrders + o;
-    const uint32_t k = s.rk[r];
-    const uint32_t pc = s.rpc[buf * 4 + i];
-    const int y = (int)(pc >> 24) & 1;
-    // bit-history walk
-    uint32_t b = bucket_of(k, L.logNS);
-    int live;
-    for (;;) {
-      const uint32_t kk = ovk[b];
-      if (kk == k + 1) {
-        live = ovs[b];
-        break;
-      }
-      if (kk == 0) {
-        live = s.rs[r];
-        ovk[b] = k + 1;
-        const int n = s.ovn[o];
-        s.ovl[n * kOrders + o] = (uint16_t)b;
-        s.ovn[o] = n + 1;
-        break;
-      }
-      b = (b + 1) & (uint32_t)(L.NS - 1);
-    }
-    ovs[b] = tab->nex[live][y];
-    // StateMap probability of the live state
-    uint32_t *sp = s.spl + live * kOrders + o;
-    const uint32_t v = *sp;
-    *sp = statep_next(v, y, tab->dt[v & 1023u]);
-    // mixer delta (Mixer::update, cucm_compress_v2.cu:663-678)
+    const int r = (rd * 4 + i) * kOrders + o;
+    k[i] = s.rk[r];
+    fz[i] = s.rs[r];
+    sm[i] = s.rsmp[r];
+    const uint32_t pc = s.rpc[rd * 4 + i];
+    y[i] = (int)(pc >> 24) & 1;
+    // mixer delta (Mixer::update, cucm_compress_v2.cu:663-678): integer adds
+    // commute, and a shared-memory reduction needs no result
     const int pr = (int)(pc & 0xffffu);
     const int cx = (int)(pc >> 16) & 0xff;
-    const int err = ((y << 12) - pr) * 7;
-    s.dw[cx * kOrders + o] += (int)(((long long)err * s.rsmp[r]) >> 16);
+    atomicAdd(s.dw + cx * kOrders + o, (int)(((long long)(((y[i] << 12) - pr) * 7) * sm[i]) >> 16));
+    b[i] = bucket_of(k[i], L.logNS);
+  }
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++) {
+    e[i] = ovk[b[i]];
+    os[i] = ovs[b[i]];
+  }
+  // slots and live states, in bit order
+  int live[4], ns[4];
+  bool fresh[4];
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++) {
+    bool same = false;
+    int lv = 0;
+CUCM_UNROLL
+    for (int j = 0; j < i; j++)
+      if (k[j] == k[i]) {
+        same = true;
+        lv = ns[j];
+        b[i] = b[j];
+      }
+    fresh[i] = false;
+    if (!same) {
+      bool taken = false;  // the bucket went to another key of this round
+CUCM_UNROLL
+      for (int j = 0; j < i; j++) taken |= (fresh[j] && b[j] == b[i]);
+      if (!taken && e[i] == k[i] + 1) {
+        lv = os[i];
+      } else if (!taken && e[i] == 0) {
+        lv = fz[i];
+        fresh[i] = true;
+      } else {
+        // collision: walk the table, skipping entries this round claims
+        uint32_t bi = b[i];
+        for (;;) {
+          bi = (bi + 1) & mask;
+          bool mine = false;
+CUCM_UNROLL
+          for (int j = 0; j < i; j++) mine |= (fresh[j] && b[j] == bi);
+          if (mine) continue;
+          const uint32_t kk = ovk[bi];
+          if (kk == k[i] + 1) {
+            lv = ovs[bi];
+            break;
+          }
+          if (kk == 0) {
+            lv = fz[i];
+            fresh[i] = true;
+            break;
+          }
+        }
+        b[i] = bi;
+      }
+    }
+    live[i] = lv;
+    ns[i] = tab->nex[lv][y[i]];
+  }
+  // StateMap probabilities of the live states: a state met m times earlier
+  // in the round has count min(count + m, 1023), so every dt is read up front
+  uint32_t v0[4], dtv[4];
+  int m[4];
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++) {
+    v0[i] = s.spl[live[i] * kOrders + o];
+    m[i] = 0;
+CUCM_UNROLL
+    for (int j = 0; j < i; j++) m[i] += (live[j] == live[i]);
+    const uint32_t c = (v0[i] & 1023u) + (uint32_t)m[i];
+    dtv[i] = tab->dt[c > 1023u ? 1023u : c];
+  }
+  uint32_t nv[4];
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++) {
+    uint32_t v = v0[i];
+CUCM_UNROLL
+    for (int j = 0; j < i; j++)
+      if (live[j] == live[i]) v = nv[j];
+    nv[i] = statep_next(v, y[i], dtv[i]);
+  }
+  // writes, in bit order
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++) {
+    if (fresh[i]) {
+      ovk[b[i]] = k[i] + 1;
+      s.ovl[nov * kOrders + o] = (uint16_t)b[i];
+      nov++;
+    }
+    ovs[b[i]] = (uint8_t)ns[i];
+    s.spl[live[i] * kOrders + o] = nv[i];
   }
 }
 
-// Unit end: overlay -> slot tables (and cleared), live probabilities become
-// frozen, deltas join the weights, the unit's bytes go out.
+// Unit end, both warps of the pair (t = 0..63): overlay -> slot tables (and
+// cleared), live probabilities become frozen, deltas join the weights, the
+// unit's bytes go out.  Called between two pair barriers.
 __device__ inline void dec_unit_end(const DecSmem &s, const DecLayout &L, uint8_t *slot, uint8_t *out, int nbytes,
-                                    int lane) {
-  __syncwarp();
+                                    int t) {
 CUCM_UNROLL
   for (int o = 0; o < kOrders; o++) {
     const int n = s.ovn[o];
     uint8_t *tb = slot + table_offset(o);
-    for (int e = lane; e < n; e += 32) {
+    for (int e = t; e < n; e += 64) {
       const int b = s.ovl[e * kOrders + o];
       const uint32_t kk = s.ovk[o * L.NS + b];
       tb[kk - 1] = s.ovs[o * L.NS + b];
       s.ovk[o * L.NS + b] = 0;
     }
   }
-  {
-    const uint4 *src = reinterpret_cast<const uint4 *>(s.spl);
-    uint4 *dst = reinterpret_cast<uint4 *>(s.spf);
-    for (int i = lane; i < 256 * kOrders / 4; i += 32) dst[i] = src[i];
-    int4 *w4 = reinterpret_cast<int4 *>(s.w);
-    int4 *d4 = reinterpret_cast<int4 *>(s.dw);
-    for (int i = lane; i < kMixCtx * kOrders / 4; i += 32) {
-      int4 a = w4[i];
-      const int4 d = d4[i];
-      a.x += d.x;
-      a.y += d.y;
-      a.z += d.z;
-      a.w += d.w;
-      w4[i] = a;
-      d4[i] = make_int4(0, 0, 0, 0);
-    }
+  const uint4 *src = reinterpret_cast<const uint4 *>(s.spl);
+  uint4 *dst = reinterpret_cast<uint4 *>(s.spf);
+  for (int i = t; i < 256 * kOrders / 4; i += 64) dst[i] = src[i];
+  int4 *w4 = reinterpret_cast<int4 *>(s.w);
+  int4 *d4 = reinterpret_cast<int4 *>(s.dw);
+  for (int i = t; i < kMixCtx * kOrders / 4; i += 64) {
+    int4 a = w4[i];
+    const int4 d = d4[i];
+    a.x += d.x;
+    a.y += d.y;
+    a.z += d.z;
+    a.w += d.w;
+    w4[i] = a;
+    d4[i] = make_int4(0, 0, 0, 0);
   }
-  if (lane < nbytes) out[lane] = s.outb[lane];
-  __syncwarp();
-  if (lane < kOrders) s.ovn[lane] = 0;
-  __syncwarp();
+  if (t < nbytes) out[t] = s.outb[t];
 }
 
-__device__ void decompress_warp_one(const ChunkTask &t, uint8_t *slot, const DecSmem &s, const Tables *tab,
-                                    const DecLayout &L, const ModelInit *init) {
+// The pair's barrier: named barrier 1 + pair index, 64 threads.
+__device__ __forceinline__ void pair_sync(int pair) {
+  asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
+}
+
+// One chunk.  role 0 decodes, role 1 updates the model; lane = threadIdx & 31.
+__device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const DecSmem &s, const Tables *tab,
+                                    const DecLayout &L, const ModelInit *init, int role, int pair,
+                                    uint32_t *status) {
   const int lane = threadIdx.x & 31;
+  const int t64 = lane + 32 * role;
   const int U = L.U;
   const uint64_t len = t.out_cap < t.cs ? t.out_cap : t.cs;  // bytes to decode
   const uint64_t nbits = 8ull * len;
   const uint8_t *pay = t.in;
   const uint64_t plen = t.in_len;
 
-  for (int i = lane; i < 256 * kOrders; i += 32) {
+  for (int i = t64; i < 256 * kOrders; i += 64) {
     const uint32_t v = init->statep[i & 7][i >> 3];
     s.spf[i] = v;
     s.spl[i] = v;
   }
-  for (int i = lane; i < kMixCtx * kOrders; i += 32) {
+  for (int i = t64; i < kMixCtx * kOrders; i += 64) {
     s.w[i] = init->w[i];
     s.dw[i] = 0;
   }
-  for (int i = lane; i < kOrders * L.NS; i += 32) s.ovk[i] = 0;
-  if (lane < kOrders) s.ovn[lane] = 0;
+  for (int i = t64; i < kOrders * L.NS; i += 64) s.ovk[i] = 0;
+  if (t64 < kOrders) s.ovn[t64] = 0;
+  if (t64 == 0) s.prog[0] = 0;
+  pair_sync(pair);
+
+  if (role == 1) {
+    // the updating warp: rounds in order, as the decoding warp publishes them
+    uint32_t done = 0;
+    bool ok = true;
+    for (uint64_t base = 0; base < nbits; base += (uint64_t)U) {
+      const int nunit = (int)(nbits - base < (uint64_t)U ? nbits - base : (uint64_t)U);
+      int nov = 0;
+      for (int rd = 0; rd < (nunit >> 2); rd++) {
+        uint32_t spins = 0;
+        while (ok && s.prog[0] <= done) {
+          if (++spins >= kDecSpinLimit) ok = false;
+          __nanosleep(64);
+        }
+        __threadfence_block();
+        if (!ok) break;
+        if (lane < kOrders) dec_update_round(s, tab, L, lane, rd, nov);
+        done++;
+      }
+      if (lane < kOrders) s.ovn[lane] = nov;
+      if (!ok && lane == 0) atomicOr(status, (uint32_t)kDevTimeout);
+      pair_sync(pair);
+      dec_unit_end(s, L, slot, t.out + (base >> 3), nunit >> 3, t64);
+      pair_sync(pair);
+    }
+    return;
+  }
+
   long long wbase = dec_refill(s.win, pay, plen, 0, lane);
 
   // coder state, identical in every lane (cucm_decompress_v2.cu:967-972)
@@ -245,7 +362,7 @@ __device__ void decompress_warp_one(const ChunkTask &t, uint8_t *slot, const Dec
   uint64_t hist = 0;  // completed bytes, most recent in the low byte
   uint32_t cur = 0;   // bits of the current byte
   int r = 0;          // 0 or 4
-  int rounds_done = 0;
+  uint32_t published = 0;
 
   for (uint64_t base = 0; base < nbits; base += (uint64_t)U) {
     const int nunit = (int)(nbits - base < (uint64_t)U ? nbits - base : (uint64_t)U);
@@ -260,8 +377,6 @@ __device__ void decompress_warp_one(const ChunkTask &t, uint8_t *slot, const Dec
       uint32_t st[kOrders];
 CUCM_UNROLL
       for (int o = 0; o < kOrders; o++) st[o] = __ldcg(slot + table_offset(o) + kk.k[o]);
-      // model update of the previous round while the gathers are in flight
-      if (rd > 0 && lane < kOrders) dec_update_round(s, tab, L, lane, (rounds_done - 1) & 1);
       // stretch, mixer context, mixer output (cucm_decompress_v2.cu:774-809)
       const int c1 = (int)(hist & 0xffu);
       int smp[kOrders];
@@ -291,26 +406,24 @@ CUCM_UNROLL
         nib = (nib << 1) | (uint32_t)y;
         n = 2 * n + 1 + y;
       }
-      // the path's lanes record their bit for the model update
-      const int buf = rounds_done & 1;
+      // the path's lanes record their bit for the updating warp
       if (recorder && pbits == (nib >> (4 - depth))) {
         const int i = depth;
-        uint4 *k4 = reinterpret_cast<uint4 *>(s.rk + (buf * 4 + i) * kOrders);
+        uint4 *k4 = reinterpret_cast<uint4 *>(s.rk + (rd * 4 + i) * kOrders);
         k4[0] = make_uint4(kk.k[0], kk.k[1], kk.k[2], kk.k[3]);
         k4[1] = make_uint4(kk.k[4], kk.k[5], kk.k[6], kk.k[7]);
         uint2 sv;
         sv.x = st[0] | (st[1] << 8) | (st[2] << 16) | (st[3] << 24);
         sv.y = st[4] | (st[5] << 8) | (st[6] << 16) | (st[7] << 24);
-        *reinterpret_cast<uint2 *>(s.rs + (buf * 4 + i) * kOrders) = sv;
+        *reinterpret_cast<uint2 *>(s.rs + (rd * 4 + i) * kOrders) = sv;
         uint4 m;
         m.x = (uint32_t)(smp[0] & 0xffff) | ((uint32_t)smp[1] << 16);
         m.y = (uint32_t)(smp[2] & 0xffff) | ((uint32_t)smp[3] << 16);
         m.z = (uint32_t)(smp[4] & 0xffff) | ((uint32_t)smp[5] << 16);
         m.w = (uint32_t)(smp[6] & 0xffff) | ((uint32_t)smp[7] << 16);
-        *reinterpret_cast<uint4 *>(s.rsmp + (buf * 4 + i) * kOrders) = m;
-        s.rpc[buf * 4 + i] = (uint32_t)pr_node | ((uint32_t)cxt << 16) | (((nib >> (3 - i)) & 1u) << 24);
+        *reinterpret_cast<uint4 *>(s.rsmp + (rd * 4 + i) * kOrders) = m;
+        s.rpc[rd * 4 + i] = (uint32_t)pr_node | ((uint32_t)cxt << 16) | (((nib >> (3 - i)) & 1u) << 24);
       }
-      rounds_done++;
       cur = (cur << 4) | nib;
       r += 4;
       if (r == 8) {
@@ -321,50 +434,61 @@ CUCM_UNROLL
         r = 0;
       }
       __syncwarp();
+      published++;
+      if (lane == 0) {
+        __threadfence_block();
+        s.prog[0] = published;
+      }
     }
-    if (lane < kOrders) dec_update_round(s, tab, L, lane, (rounds_done - 1) & 1);
-    dec_unit_end(s, L, slot, t.out + (base >> 3), nunit >> 3, lane);
+    pair_sync(pair);
+    dec_unit_end(s, L, slot, t.out + (base >> 3), nunit >> 3, t64);
+    pair_sync(pair);
   }
 }
 
-__global__ void __launch_bounds__(kDecMaxWarps * 32)
-    decompress_warp_kernel(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
+// Grid: chunk slots in pairs of warps; warp 2c decodes chunk slot c of the
+// CTA, warp 2c + 1 updates its model.
+__global__ void __launch_bounds__(kDecMaxPairs * 64)
+    decompress_pair_kernel(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                            const uint8_t *init_tables, const ModelInit *init, uint32_t *queue, uint32_t *status,
                            int unit) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  const int warps = blockDim.x >> 5;
-  const DecLayout L = make_dec_layout(unit, warps);
+  const int pairs = blockDim.x >> 6;
+  const DecLayout L = make_dec_layout(unit, pairs);
   Tables *tab = reinterpret_cast<Tables *>(smem_raw + L.off_tab);
   copy_tables(&g_tables, tab);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t gw = blockIdx.x * (uint32_t)warps + (uint32_t)warp;
-  if (gw >= nslots) return;
-  const DecSmem s = carve_dec(smem_raw, L, warp);
-  uint8_t *slot = slots + (size_t)gw * kSlotTableBytes;
+  const int pair = warp >> 1, role = warp & 1;
+  const uint32_t gs = blockIdx.x * (uint32_t)pairs + (uint32_t)pair;
+  if (gs >= nslots) return;  // both warps of the pair leave together
+  const DecSmem s = carve_dec(smem_raw, L, pair);
+  uint8_t *slot = slots + (size_t)gs * kSlotTableBytes;
   bool fresh = true;
   for (;;) {
-    uint32_t ti = 0;
-    if (lane == 0) ti = atomicAdd(queue, 1u);
-    ti = __shfl_sync(0xffffffffu, ti, 0);
+    if (role == 0 && lane == 0) s.prog[1] = atomicAdd(queue, 1u);
+    pair_sync(pair);
+    const uint32_t ti = s.prog[1];
+    pair_sync(pair);
     if (ti >= ntasks) break;
     const ChunkTask t = tasks[ti];
     if (t.unit != (uint32_t)unit || t.cs == 0) {
-      if (lane == 0) atomicOr(status, (uint32_t)kDevBadTask);
+      if (role == 0 && lane == 0) atomicOr(status, (uint32_t)kDevBadTask);
       continue;
     }
     if (!fresh) {
       uint4 *d = reinterpret_cast<uint4 *>(slot);
       const size_t nv = kSlotTableBytes / 16;
+      const int t64 = lane + 32 * role;
       if (init_tables) {
         const uint4 *src = reinterpret_cast<const uint4 *>(init_tables);
-        for (size_t i = lane; i < nv; i += 32) d[i] = src[i];
+        for (size_t i = t64; i < nv; i += 64) d[i] = src[i];
       } else {
-        for (size_t i = lane; i < nv; i += 32) d[i] = make_uint4(0, 0, 0, 0);
+        for (size_t i = t64; i < nv; i += 64) d[i] = make_uint4(0, 0, 0, 0);
       }
-      __syncwarp();
+      pair_sync(pair);
     }
     fresh = false;
-    decompress_warp_one(t, slot, s, tab, L, init);
+    decompress_pair_one(t, slot, s, tab, L, init, role, pair, status);
   }
 }

@@ -33,6 +33,7 @@ enum DevStatus : uint32_t {
   kDevOk = 0,
   kDevOverflow = 1,      // some chunk's payload exceeded its scratch capacity
   kDevBadTask = 2,       // malformed task (unit/size out of range)
+  kDevTimeout = 4,       // a bounded wait between the warps of a chunk gave up
 };
 
 struct EngineConfig {

@@ -579,18 +579,18 @@ cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *
   return cudaGetLastError();
 }
 
-// Chunk warps of the one-warp decoder that fit in one CTA's shared memory.
-static int dec_max_warps(int unit) {
+// Chunks (warp pairs) of the decoder that fit in one CTA's shared memory.
+static int dec_max_pairs(int unit) {
   const DecLayout one = make_dec_layout(unit, 1);
   const size_t avail = 227 * 1024 - (one.total - one.per_warp);
   int w = (int)(avail / one.per_warp);
-  return w < 1 ? 1 : (w > kDecMaxWarps ? kDecMaxWarps : w);
+  return w < 1 ? 1 : (w > kDecMaxPairs ? kDecMaxPairs : w);
 }
 
 static bool dec_fast(int unit, const EngineConfig &cfg) { return unit <= kDecMaxUnit && !cfg.generic; }
 
 int engine_slots_per_sm(bool decode, int unit, const EngineConfig &cfg) {
-  if (decode && dec_fast(unit, cfg)) return dec_max_warps(unit);
+  if (decode && dec_fast(unit, cfg)) return dec_max_pairs(unit);
   if (!decode && unit <= kFastMaxUnit && !cfg.generic) return 2;
   const size_t smem = decode ? decompress_smem_bytes(unit, cfg.spec_bits) : make_layout(unit, 0).total;
   return smem > 110 * 1024 ? 1 : (smem > 72 * 1024 ? 2 : 3);
@@ -600,7 +600,7 @@ cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t
                               const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
                               uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit) {
   if (dec_fast(unit, cfg)) {
-    // One chunk per warp; spread the warps over all SMs before stacking them.
+    // One chunk per warp pair; spread the pairs over all SMs before stacking them.
     int sms = cfg.sm_count;
     if (sms <= 0) {
       int dev = 0;
@@ -609,14 +609,14 @@ cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t
       if (sms <= 0) sms = 1;
     }
     int wpc = (int)((nslots + (uint32_t)sms - 1) / (uint32_t)sms);
-    const int wmax = dec_max_warps(unit);
+    const int wmax = dec_max_pairs(unit);
     if (wpc > wmax) wpc = wmax;
     if (wpc < 1) wpc = 1;
     const DecLayout L = make_dec_layout(unit, wpc);
-    cudaError_t e = set_smem((const void *)decompress_warp_kernel, L.total);
+    cudaError_t e = set_smem((const void *)decompress_pair_kernel, L.total);
     if (e != cudaSuccess) return e;
     const uint32_t grid = (nslots + (uint32_t)wpc - 1) / (uint32_t)wpc;
-    decompress_warp_kernel<<<grid, wpc * 32, L.total, stream>>>(d_tasks, ntasks, slots, nslots, init_tables, d_init,
+    decompress_pair_kernel<<<grid, wpc * 64, L.total, stream>>>(d_tasks, ntasks, slots, nslots, init_tables, d_init,
                                                                 d_queue, d_status, unit);
     return cudaGetLastError();
   }

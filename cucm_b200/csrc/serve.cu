@@ -441,6 +441,7 @@ int start_launch(cucm_server *s, std::vector<Req *> &grp, uint32_t slot0, uint32
 // Decompress launch whose kernel is done: outputs back to the callers.
 int after_decode(cucm_server *s, Launch *l) {
   if (*l->h_status & kDevBadTask) return CUCM_EFORMAT;
+  if (*l->h_status & kDevTimeout) return CUCM_ETIMEOUT;
   for (size_t j = 0; j < l->reqs.size(); j++) {
     Req *r = l->reqs[j];
     if (r->out_body)
