@@ -77,6 +77,17 @@ def dist_env():
     return rank, world, local
 
 
+def reduce_max(vals, dist=None, device="cpu"):
+    """Element-wise max over ranks of per-rank figures (the slowest rank's
+    device times); the identity without a process group."""
+    if dist is None:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -323,10 +334,7 @@ def main():
         launches += sc["launches"] + sd["launches"]
     barrier()
     clocks = sampler.stop()
-    tot = torch.tensor([tc + td, tc, td], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    t_all, t_c, t_d = [float(x) for x in tot.tolist()]
+    t_all, t_c, t_d = reduce_max([tc + td, tc, td], dist, dev)
     K = max(args.steps, 1)
     total_bytes = world * n * K
     value = total_bytes / (t_all / 1e3) / 1e6
@@ -358,10 +366,8 @@ def main():
                 d2h += m + n
         if not torch.equal(h_back, h_in):
             raise SystemExit("host round trip mismatch")
-        et = torch.tensor([e_ms], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * n * K / (float(et.item()) / 1e3) / 1e6, "unit": "MB/s",
+        e_max = reduce_max([e_ms], dist, dev)[0]
+        e2e = {"value": world * n * K / (e_max / 1e3) / 1e6, "unit": "MB/s",
                "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K}
 
     if rank != 0:
