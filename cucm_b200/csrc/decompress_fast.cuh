@@ -388,13 +388,21 @@ CUCM_UNROLL
       }
       const int cxt = olen + (c1 >> 5) * 10;
       const int pr_node = mix_pr(s.w, cxt, smp, tab);
-      // decode 4 bits along the tree (cucm_decompress_v2.cu:813-868)
+      // decode 4 bits along the tree (cucm_decompress_v2.cu:813-868); both
+      // children's split factors are fetched while a bit is decided, so the
+      // shuffle is off the bit-to-bit chain
+      const uint32_t f_node = (uint32_t)pr_node << 20;
       int n = 0;
       uint32_t nib = 0;
+      uint32_t f = __shfl_sync(0xffffffffu, f_node, 0);
 CUCM_UNROLL
       for (int i = 0; i < 4; i++) {
-        const uint32_t pr = (uint32_t)__shfl_sync(0xffffffffu, pr_node, n);
-        const uint32_t xm = x1 + __umulhi(x2 - x1, pr << 20);
+        uint32_t fa = 0, fb = 0;
+        if (i < 3) {
+          fa = __shfl_sync(0xffffffffu, f_node, 2 * n + 1);
+          fb = __shfl_sync(0xffffffffu, f_node, 2 * n + 2);
+        }
+        const uint32_t xm = x1 + __umulhi(x2 - x1, f);
         const int y = x <= xm;
         if (y) x2 = xm; else x1 = xm + 1;
         while ((x1 ^ x2) < 0x1000000u) {
@@ -405,6 +413,7 @@ CUCM_UNROLL
         }
         nib = (nib << 1) | (uint32_t)y;
         n = 2 * n + 1 + y;
+        f = y ? fb : fa;
       }
       // the path's lanes record their bit for the updating warp
       if (recorder && pbits == (nib >> (4 - depth))) {
