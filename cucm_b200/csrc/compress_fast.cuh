@@ -216,79 +216,158 @@ __device__ __forceinline__ int slot_find(const uint32_t *row, int logNBK, uint32
 }
 
 // Front: slots of unit v in its own table, and in the previous unit's.
+// Front warp w owns orders 2w and 2w + 1, so no other warp writes its rows;
+// a step takes two bytes, lane = (order, bit, byte).  A lane whose key is
+// not yet in the table either follows a lane of the step with the same key
+// (a slot recurs at most once per byte) or, as the key's leader, takes the
+// next free place of its bucket after the leaders before it in the same
+// bucket (warp match and rank, no atomics).  Leaders that find their bucket
+// full move on to the next bucket and rank again.
 __device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
   const int U = L.U, NS = L.NSLOT;
-  const int n = kOrders * U;
   uint32_t *hk = s.hk + (v & 1) * kOrders * NS;
   const uint32_t *hk_prev = s.hk + ((v + 1) & 1) * kOrders * NS;
   const uint32_t *key = s.key + (v & 1) * kOrders * U;
   uint16_t *lnk = s.lnk + (v & 1) * kOrders * U;
   uint16_t *bkt = s.bkt + (v & 1) * kOrders * U;
+  const int lane = t & 31, w = t >> 5;
+  const int o = 2 * w + (lane >> 4), r = (lane >> 1) & 7, half = lane & 1;
+  uint32_t *row = hk + o * NS;
+  const uint32_t *prow = hk_prev + o * NS;
+  const uint32_t nbk_mask = (uint32_t)L.NSLOT / 4 - 1;
   {
-    uint4 *k4 = reinterpret_cast<uint4 *>(hk);
+    // this warp's two rows
+    uint4 *k4 = reinterpret_cast<uint4 *>(hk + 2 * w * NS);
     const uint4 z = make_uint4(0, 0, 0, 0);
-    for (int i = t; i < kOrders * NS / 4; i += kFrontThreads) k4[i] = z;
+    for (int i = lane; i < 2 * NS / 4; i += 32) k4[i] = z;
+    __syncwarp();
   }
-  front_sync();
-  for (int e = t; e < n; e += kFrontThreads) {
-    const int j = e >> 3, o = e & 7;
-    if (j >= nvalid) continue;
-    const uint32_t kp = key[e] + 1;
-    bkt[e] = (uint16_t)slot_insert(hk + o * NS, L.logNBK, kp);
-    lnk[e] = (uint16_t)(slot_find(hk_prev + o * NS, L.logNBK, kp) + 1);
+  const unsigned lt = (1u << lane) - 1u;
+  for (int q0 = 0; q0 < (nvalid >> 3); q0 += 2) {
+    const int q = q0 + half;
+    const bool valid = q < (nvalid >> 3);
+    const int idx = (q * 8 + r) * kOrders + o;
+    const uint32_t kp = valid ? key[idx] + 1 : 0u;
+    // cross-unit link: the previous unit's table is read-only here
+    if (valid) lnk[idx] = (uint16_t)(slot_find(prow, L.logNBK, kp) + 1);
+    // this unit's slot
+    uint32_t b = bucket_of(kp - 1, L.logNBK);
+    int slot_id = -1;
+    bool pending = valid;
+    // lanes with the same key (and order) in this step share one slot
+    const unsigned same = __match_any_sync(0xffffffffu, valid ? ((uint32_t)o << 25 | (kp - 1)) : 0xffffffffu);
+    const bool leader = valid && (same & lt) == 0;
+    const int lead = __ffs(same) - 1;
+    while (__any_sync(0xffffffffu, pending)) {
+      uint4 qb = make_uint4(1, 1, 1, 1);
+      if (pending) qb = *reinterpret_cast<const uint4 *>(row + 4 * b);
+      if (pending) {
+        if (qb.x == kp) slot_id = 4 * b;
+        else if (qb.y == kp) slot_id = 4 * b + 1;
+        else if (qb.z == kp) slot_id = 4 * b + 2;
+        else if (qb.w == kp) slot_id = 4 * b + 3;
+        if (slot_id >= 0) pending = false;
+      }
+      // leaders still without a slot claim a free place of their bucket
+      const bool claim = pending && leader;
+      const unsigned mb = __match_any_sync(0xffffffffu, claim ? ((uint32_t)o << 8 | b) : 0xffffffffu);
+      if (claim) {
+        const int used = (qb.x != 0) + (qb.y != 0) + (qb.z != 0) + (qb.w != 0);
+        const int pos = used + __popc(mb & lt);
+        if (pos < 4) {
+          row[4 * b + pos] = kp;
+          slot_id = 4 * b + pos;
+          pending = false;
+        } else {
+          b = (b + 1) & nbk_mask;
+        }
+      }
+      __syncwarp();
+      // followers take their leader's slot once it has one
+      const int ls = __shfl_sync(0xffffffffu, slot_id, lead);
+      if (pending && !leader && ls >= 0) {
+        slot_id = ls;
+        pending = false;
+      }
+    }
+    if (valid) bkt[idx] = (uint16_t)slot_id;
   }
 }
 
-// Walker (lane = order): bit-history updates of unit v in bit order.
-__device__ __forceinline__ void walk_unit(const FastSmem &s, const FastLayout &L, uint8_t *slot, int o, int v,
+// Walker: bit-history updates of unit v in bit order, a byte per step.  A
+// slot recurs at most once per byte except when two keys of one order
+// collide in the 25-bit hash, so the 64 updates of a byte (lane: order
+// lane & 7, bits lane >> 3 and (lane >> 3) + 4) are independent and run
+// together; a byte with a collision is walked bit by bit instead.  Per
+// update: the state it sees (live: an earlier touch in this unit, else the
+// frozen unit-start state -- from the previous unit's table when linked),
+// the next state, written through to the slot table.  It only depends on
+// the bits, never on the probabilities, so it runs a unit ahead of the
+// chain.
+__device__ __forceinline__ void walk_unit(const FastSmem &s, const FastLayout &L, uint8_t *slot, int lane, int v,
                                           int n) {
   const int U = L.U, NS = L.NSLOT;
-  const uint32_t *hk = s.hk + ((v & 1) * kOrders + o) * NS;  // this unit's slots: key + 1
-  const uint16_t *lnk = s.lnk + (v & 1) * U * kOrders + o;   // interleaved by order: 8 lanes, 8 banks
-  const uint16_t *bkt = s.bkt + (v & 1) * U * kOrders + o;
-  const uint8_t *fsb = s.fsw + (v & 1) * U * kOrders + o;
+  const int o = lane & 7, r0 = lane >> 3;
+  const uint32_t *hk = s.hk + ((v & 1) * kOrders + o) * NS;
+  const uint16_t *lnk = s.lnk + (v & 1) * U * kOrders;
+  const uint16_t *bkt = s.bkt + (v & 1) * U * kOrders;
+  const uint8_t *fsb = s.fsw + (v & 1) * U * kOrders;
   const uint32_t *yw = s.yw + (v & 3) * (U / 32);
-  uint8_t *st = s.st + (v & 1) * U * kOrders + o;
-  uint8_t *fr = s.fr + (v & 1) * U * kOrders + o;
+  uint8_t *st = s.st + (v & 1) * U * kOrders;
+  uint8_t *fr = s.fr + (v & 1) * U * kOrders;
   uint16_t *ns_cur = s.ns + ((v & 1) * kOrders + o) * NS;
   const uint16_t *ns_prev = s.ns + (((v + 1) & 1) * kOrders + o) * NS;
   uint8_t *tab = slot + table_offset(o);
   const Tables *tb = s.tab;
-  // Software pipeline: what step j+1 reads and step j does not write is
-  // loaded before step j's stores; the slot's latest state (the one value
-  // step j can change) is forwarded when the slots are equal.
-  auto fetch = [&](int j, int &b, uint32_t &frz, uint32_t &kp, uint32_t &nc) {
-    const uint32_t cross = lnk[j * kOrders];
-    b = bkt[j * kOrders];
-    frz = cross ? (uint32_t)(ns_prev[cross - 1] & 0xffu) : (uint32_t)fsb[j * kOrders];
-    kp = hk[b];
-    nc = ns_cur[b];
-  };
-  int b = 0;
-  uint32_t frz = 0, kp = 0, nc = 0;
-  if (n > 0) fetch(0, b, frz, kp, nc);
-  uint32_t ywd = 0;
-  int prev_b = -1;
-  uint32_t prev_ns = 0;
-  for (int j = 0; j < n; j++) {
-    int b1 = 0;
-    uint32_t frz1 = 0, kp1 = 0, nc1 = 0;
-    if (j + 1 < n) fetch(j + 1, b1, frz1, kp1, nc1);
-    if ((j & 31) == 0) ywd = yw[j >> 5];
-    const uint32_t y = (ywd >> (j & 31)) & 1u;
-    uint32_t live = (nc & 0x100u) ? (nc & 0xffu) : frz;  // earlier touch of the slot in this unit
-    if (b == prev_b) live = prev_ns;
-    const uint32_t ns = tb->nex[live][y];
-    ns_cur[b] = (uint16_t)(0x100u | ns);
-    st[j * kOrders] = (uint8_t)live;
-    fr[j * kOrders] = (uint8_t)frz;
-    tab[kp - 1] = (uint8_t)ns;  // write-through; later touches of the slot overwrite it
-    prev_b = b;
-    prev_ns = ns;
-    b = b1;
-    frz = frz1;
-    kp = kp1;
-    nc = nc1;
+  for (int q = 0; q < (n >> 3); q++) {
+    const int ja = q * 8 + r0, jb = ja + 4;
+    const int ia = ja * kOrders + o, ib = jb * kOrders + o;
+    const uint32_t ba = bkt[ia], bb = bkt[ib];
+    // the byte's 8 slots of this order: any two alike?
+    bool clash = ba == bb;
+CUCM_UNROLL
+    for (int k = 0; k < 4; k++) {
+      const uint32_t oa = __shfl_sync(0xffffffffu, ba, k * 8 + o);
+      const uint32_t ob = __shfl_sync(0xffffffffu, bb, k * 8 + o);
+      clash |= (k != r0) && (oa == ba || ob == ba || oa == bb || ob == bb);
+    }
+    if (!__any_sync(0xffffffffu, clash)) {
+      const uint32_t ca = lnk[ia], cb = lnk[ib];
+      const uint32_t fa = ca ? (uint32_t)(ns_prev[ca - 1] & 0xffu) : (uint32_t)fsb[ia];
+      const uint32_t fb = cb ? (uint32_t)(ns_prev[cb - 1] & 0xffu) : (uint32_t)fsb[ib];
+      const uint32_t na = ns_cur[ba], nb = ns_cur[bb];
+      const uint32_t ka = hk[ba], kb = hk[bb];
+      const uint32_t yword = yw[q >> 2];
+      const uint32_t ya = (yword >> (ja & 31)) & 1u, yb = (yword >> (jb & 31)) & 1u;
+      const uint32_t la = (na & 0x100u) ? (na & 0xffu) : fa;
+      const uint32_t lb = (nb & 0x100u) ? (nb & 0xffu) : fb;
+      const uint32_t sa = tb->nex[la][ya], sb = tb->nex[lb][yb];
+      ns_cur[ba] = (uint16_t)(0x100u | sa);
+      ns_cur[bb] = (uint16_t)(0x100u | sb);
+      st[ia] = (uint8_t)la;
+      st[ib] = (uint8_t)lb;
+      fr[ia] = (uint8_t)fa;
+      fr[ib] = (uint8_t)fb;
+      tab[ka - 1] = (uint8_t)sa;  // write-through; later touches overwrite it
+      tab[kb - 1] = (uint8_t)sb;
+    } else if (lane < kOrders) {
+      // bit by bit for this byte, lane = order
+      for (int r = 0; r < 8; r++) {
+        const int j = q * 8 + r, i = j * kOrders + lane;
+        const uint32_t b = bkt[i];
+        const uint32_t c = lnk[i];
+        const uint32_t f = c ? (uint32_t)(ns_prev[c - 1] & 0xffu) : (uint32_t)fsb[i];
+        const uint32_t nc = ns_cur[b];
+        const uint32_t y = (yw[j >> 5] >> (j & 31)) & 1u;
+        const uint32_t lv = (nc & 0x100u) ? (nc & 0xffu) : f;
+        const uint32_t ns = tb->nex[lv][y];
+        ns_cur[b] = (uint16_t)(0x100u | ns);
+        st[i] = (uint8_t)lv;
+        fr[i] = (uint8_t)f;
+        tab[hk[b] - 1] = (uint8_t)ns;
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -489,7 +568,7 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
         uint4 *z4 = reinterpret_cast<uint4 *>(s.ns + (tau & 1) * kOrders * L.NSLOT);
         for (int i = lane; i < kOrders * L.NSLOT / 8; i += 32) z4[i] = make_uint4(0, 0, 0, 0);
         __syncwarp();
-        if (lane < kOrders) walk_unit(s, L, slot, lane, tau, fast_nvalid(data_bits, U, tau));
+        walk_unit(s, L, slot, lane, tau, fast_nvalid(data_bits, U, tau));
       }
     } else {
       if (um >= 0 && um < nU) front_mix(s, L, ft, um, fast_nvalid(data_bits, U, um));

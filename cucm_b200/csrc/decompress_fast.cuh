@@ -148,6 +148,7 @@ __device__ __forceinline__ void dec_update_round(const DecSmem &s, const Tables 
   const uint32_t mask = (uint32_t)(L.NS - 1);
   uint32_t k[4], b[4], e[4];
   int fz[4], sm[4], y[4], os[4];
+  int cx[4], dl[4];
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) {
     const int r = (rd * 4 + i) * kOrders + o;
@@ -156,13 +157,27 @@ CUCM_UNROLL
     sm[i] = s.rsmp[r];
     const uint32_t pc = s.rpc[rd * 4 + i];
     y[i] = (int)(pc >> 24) & 1;
-    // mixer delta (Mixer::update, cucm_compress_v2.cu:663-678): integer adds
-    // commute, and a shared-memory reduction needs no result
     const int pr = (int)(pc & 0xffffu);
-    const int cx = (int)(pc >> 16) & 0xff;
-    atomicAdd(s.dw + cx * kOrders + o, (int)(((long long)(((y[i] << 12) - pr) * 7) * sm[i]) >> 16));
+    cx[i] = (int)(pc >> 16) & 0xff;
+    dl[i] = (int)(((long long)(((y[i] << 12) - pr) * 7) * sm[i]) >> 16);
     b[i] = bucket_of(k[i], L.logNS);
   }
+  // mixer deltas (Mixer::update, cucm_compress_v2.cu:663-678): this lane
+  // alone owns column o of the delta rows; deltas of the round's bits that
+  // share a row are summed first (integer adds commute), then every distinct
+  // row is read and written once
+  bool merged[4] = {false, false, false, false};
+CUCM_UNROLL
+  for (int i = 1; i < 4; i++)
+CUCM_UNROLL
+    for (int j = 0; j < i; j++)
+      if (!merged[i] && !merged[j] && cx[j] == cx[i]) {
+        dl[j] += dl[i];
+        merged[i] = true;
+      }
+  int dv[4];
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++) dv[i] = s.dw[cx[i] * kOrders + o];
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) {
     e[i] = ovk[b[i]];
@@ -241,6 +256,9 @@ CUCM_UNROLL
     nv[i] = statep_next(v, y[i], dtv[i]);
   }
   // writes, in bit order
+CUCM_UNROLL
+  for (int i = 0; i < 4; i++)
+    if (!merged[i]) s.dw[cx[i] * kOrders + o] = dv[i] + dl[i];
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) {
     if (fresh[i]) {
