@@ -35,7 +35,7 @@ constexpr int kDecMaxPairs = 8;          // chunks per CTA
 constexpr int kDecWin = 2048;            // payload window per chunk (bytes)
 constexpr int kDecNodes = 15;            // nodes of a 4-bit speculation tree
 constexpr int kDecRecBytes = 240;        // one round's records
-constexpr uint32_t kDecSpinLimit = 1u << 26;  // bound of the updater's wait for a round
+constexpr uint32_t kDecSpinLimit = 1u << 27;  // polls bounding the updater's wait for a round (seconds)
 
 struct DecLayout {
   int U, NS, logNS, warps, rounds;
@@ -61,7 +61,7 @@ __host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
   L.off_spl = take(sizeof(uint32_t) * 256 * kOrders);          // live statep [state][order]
   L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);         // frozen weights
   L.off_dw = take(sizeof(int32_t) * kMixCtx * kOrders);        // summed deltas of the unit
-  L.off_ovk = take(sizeof(uint32_t) * kOrders * L.NS);         // overlay keys + 1 (0 = empty)
+  L.off_ovk = take(sizeof(uint32_t) * kOrders * L.NS);         // overlay keys + 1 (0 = empty), 4-key buckets
   L.off_ovs = take((size_t)kOrders * L.NS);                    // overlay live states
   L.off_ovl = take(sizeof(uint16_t) * U * kOrders);            // overlay entries in use [entry][order]
   L.off_ovn = take(sizeof(int) * kOrders);
@@ -130,6 +130,16 @@ __device__ inline long long dec_refill(uint8_t *win, const uint8_t *pay, uint64_
   return (long long)(a - pay);
 }
 
+// Overlay buckets hold 4 keys (+ 1, 0 = empty), filled in order and never
+// emptied within a unit; a key whose bucket is full lives in the next bucket
+// with room.  Place of `want` in bucket q, or -1:
+__device__ __forceinline__ int bucket_place(const uint4 &q, uint32_t want) {
+  return q.x == want ? 0 : q.y == want ? 1 : q.z == want ? 2 : q.w == want ? 3 : -1;
+}
+__device__ __forceinline__ int bucket_used(const uint4 &q) {
+  return (q.x != 0u) + (q.y != 0u) + (q.z != 0u) + (q.w != 0u);
+}
+
 // Model update of one round's 4 bits for order `o` (one lane per order), in
 // bit order: the live state of each slot (overlay, else the frozen state the
 // prediction saw), its next state, the StateMap probability of the live state
@@ -145,9 +155,9 @@ __device__ __forceinline__ void dec_update_round(const DecSmem &s, const Tables 
                                                  int rd, int &nov) {
   uint32_t *ovk = s.ovk + o * L.NS;
   uint8_t *ovs = s.ovs + o * L.NS;
-  const uint32_t mask = (uint32_t)(L.NS - 1);
-  uint32_t k[4], b[4], e[4];
-  int fz[4], sm[4], y[4], os[4];
+  const uint32_t bmask = (uint32_t)(L.NS / 4 - 1);
+  uint32_t k[4], b[4], e[4] = {0, 0, 0, 0};
+  int fz[4], sm[4], y[4];
   int cx[4], dl[4];
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) {
@@ -160,7 +170,7 @@ CUCM_UNROLL
     const int pr = (int)(pc & 0xffffu);
     cx[i] = (int)(pc >> 16) & 0xff;
     dl[i] = (int)(((long long)(((y[i] << 12) - pr) * 7) * sm[i]) >> 16);
-    b[i] = bucket_of(k[i], L.logNS);
+    b[i] = bucket_of(k[i], L.logNS - 2);
   }
   // mixer deltas (Mixer::update, cucm_compress_v2.cu:663-678): this lane
   // alone owns column o of the delta rows; deltas of the round's bits that
@@ -178,12 +188,17 @@ CUCM_UNROLL
   int dv[4];
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) dv[i] = s.dw[cx[i] * kOrders + o];
+  // the four bits' buckets: keys and states
+  const uint4 *ovk4 = reinterpret_cast<const uint4 *>(ovk);
+  const uint32_t *ovs4 = reinterpret_cast<const uint32_t *>(ovs);
+  uint4 q[4];
+  uint32_t qs[4];
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) {
-    e[i] = ovk[b[i]];
-    os[i] = ovs[b[i]];
+    q[i] = ovk4[b[i]];
+    qs[i] = ovs4[b[i]];
   }
-  // slots and live states, in bit order
+  // slots and live states, in bit order; e = slot (bucket * 4 + place)
   int live[4], ns[4];
   bool fresh[4];
 CUCM_UNROLL
@@ -195,39 +210,48 @@ CUCM_UNROLL
       if (k[j] == k[i]) {
         same = true;
         lv = ns[j];
-        b[i] = b[j];
+        e[i] = e[j];
       }
     fresh[i] = false;
     if (!same) {
-      bool taken = false;  // the bucket went to another key of this round
-CUCM_UNROLL
-      for (int j = 0; j < i; j++) taken |= (fresh[j] && b[j] == b[i]);
-      if (!taken && e[i] == k[i] + 1) {
-        lv = os[i];
-      } else if (!taken && e[i] == 0) {
-        lv = fz[i];
-        fresh[i] = true;
+      const uint32_t want = k[i] + 1;
+      const int hit = bucket_place(q[i], want);
+      if (hit >= 0) {
+        e[i] = b[i] * 4 + (uint32_t)hit;
+        lv = (int)(qs[i] >> (8 * hit)) & 0xff;
       } else {
-        // collision: walk the table, skipping entries this round claims
-        uint32_t bi = b[i];
-        for (;;) {
-          bi = (bi + 1) & mask;
-          bool mine = false;
+        // places this round has already claimed in the bucket
+        int used = bucket_used(q[i]);
 CUCM_UNROLL
-          for (int j = 0; j < i; j++) mine |= (fresh[j] && b[j] == bi);
-          if (mine) continue;
-          const uint32_t kk = ovk[bi];
-          if (kk == k[i] + 1) {
-            lv = ovs[bi];
-            break;
-          }
-          if (kk == 0) {
-            lv = fz[i];
-            fresh[i] = true;
-            break;
+        for (int j = 0; j < i; j++) used += (fresh[j] && (e[j] >> 2) == b[i]);
+        if (used < 4) {
+          e[i] = b[i] * 4 + (uint32_t)used;
+          lv = fz[i];
+          fresh[i] = true;
+        } else {
+          // full bucket: the key is in a later one, or goes to the first
+          // with room
+          uint32_t bi = b[i];
+          for (uint32_t it = 0; it <= bmask; it++) {
+            bi = (bi + 1) & bmask;
+            const uint4 qq = ovk4[bi];
+            const int h = bucket_place(qq, want);
+            if (h >= 0) {
+              e[i] = bi * 4 + (uint32_t)h;
+              lv = ovs[e[i]];
+              break;
+            }
+            int u = bucket_used(qq);
+CUCM_UNROLL
+            for (int j = 0; j < i; j++) u += (fresh[j] && (e[j] >> 2) == bi);
+            if (u < 4) {
+              e[i] = bi * 4 + (uint32_t)u;
+              lv = fz[i];
+              fresh[i] = true;
+              break;
+            }
           }
         }
-        b[i] = bi;
       }
     }
     live[i] = lv;
@@ -262,11 +286,11 @@ CUCM_UNROLL
 CUCM_UNROLL
   for (int i = 0; i < 4; i++) {
     if (fresh[i]) {
-      ovk[b[i]] = k[i] + 1;
-      s.ovl[nov * kOrders + o] = (uint16_t)b[i];
+      ovk[e[i]] = k[i] + 1;
+      s.ovl[nov * kOrders + o] = (uint16_t)e[i];
       nov++;
     }
-    ovs[b[i]] = (uint8_t)ns[i];
+    ovs[e[i]] = (uint8_t)ns[i];
     s.spl[live[i] * kOrders + o] = nv[i];
   }
 }
@@ -346,8 +370,9 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
       for (int rd = 0; rd < (nunit >> 2); rd++) {
         uint32_t spins = 0;
         while (ok && s.prog[0] <= done) {
+          // a plain poll: a sleep here wakes late and the updating warp
+          // falls rounds behind by the unit's end
           if (++spins >= kDecSpinLimit) ok = false;
-          __nanosleep(64);
         }
         __threadfence_block();
         if (!ok) break;
