@@ -35,18 +35,23 @@ constexpr int kDecMaxPairs = 8;          // chunks per CTA
 constexpr int kDecWin = 2048;            // payload window per chunk (bytes)
 constexpr int kDecNodes = 15;            // nodes of a 4-bit speculation tree
 constexpr int kDecRecBytes = 240;        // one round's records
+constexpr size_t kDecSmemLimit = 227 * 1024;  // dynamic shared memory of one CTA
 constexpr uint32_t kDecSpinLimit = 1u << 27;  // polls bounding the updater's wait for a round (seconds)
 
 struct DecLayout {
   int U, NS, logNS, warps, rounds;
+  bool low;  // order 0/1 tables held in shared memory
   size_t off_spf, off_spl, off_w, off_dw, off_ovk, off_ovs, off_ovl, off_ovn, off_prog, off_rk, off_rs, off_rsmp,
-      off_rpc, off_win, off_outb, per_warp, off_tab, total;
+      off_rpc, off_win, off_outb, off_t01, per_warp, off_tab, total;
 };
 
 // Shared memory of `warps` chunks (warp pairs) and the shared tables.
-__host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
+// With `low`, each chunk also holds its order 0 and 1 tables (the first
+// kHashedOff bytes of its slot, 64.25 KiB) in shared memory.
+__host__ __device__ inline DecLayout make_dec_layout(int U, int warps, bool low = false) {
   DecLayout L;
   L.U = U;
+  L.low = low;
   L.rounds = U / 4;
   L.NS = next_pow2(2 * U);  // overlay slots per order (load <= 1/2)
   L.logNS = ilog2(L.NS);
@@ -57,7 +62,7 @@ __host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
     o = (o + bytes + 15) & ~(size_t)15;
     return at;
   };
-  L.off_spf = take(sizeof(uint32_t) * 256 * kOrders);          // frozen statep [state][order]
+  L.off_spf = take(sizeof(uint16_t) * 256 * kOrders);          // frozen probability (statep >> 20) [state][order]
   L.off_spl = take(sizeof(uint32_t) * 256 * kOrders);          // live statep [state][order]
   L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);         // frozen weights
   L.off_dw = take(sizeof(int32_t) * kMixCtx * kOrders);        // summed deltas of the unit
@@ -72,6 +77,7 @@ __host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
   L.off_rpc = take(sizeof(uint32_t) * L.rounds * 4);           // pr | cxt << 16 | y << 24
   L.off_win = take((size_t)kDecWin);
   L.off_outb = take((size_t)kDecMaxUnit / 8);
+  L.off_t01 = low ? take((size_t)kHashedOff) : 0;
   L.per_warp = o;
   L.off_tab = (size_t)warps * L.per_warp;
   L.total = L.off_tab + ((sizeof(Tables) + 15) & ~(size_t)15);
@@ -79,7 +85,8 @@ __host__ __device__ inline DecLayout make_dec_layout(int U, int warps) {
 }
 
 struct DecSmem {
-  uint32_t *spf, *spl;
+  uint16_t *spf;
+  uint32_t *spl;
   int32_t *w, *dw;
   uint32_t *ovk;
   uint8_t *ovs;
@@ -91,12 +98,13 @@ struct DecSmem {
   int16_t *rsmp;
   uint32_t *rpc;
   uint8_t *win, *outb;
+  uint8_t *t01;  // order 0/1 tables, or null
 };
 
 __device__ inline DecSmem carve_dec(uint8_t *base, const DecLayout &L, int warp) {
   uint8_t *b = base + (size_t)warp * L.per_warp;
   DecSmem s;
-  s.spf = reinterpret_cast<uint32_t *>(b + L.off_spf);
+  s.spf = reinterpret_cast<uint16_t *>(b + L.off_spf);
   s.spl = reinterpret_cast<uint32_t *>(b + L.off_spl);
   s.w = reinterpret_cast<int32_t *>(b + L.off_w);
   s.dw = reinterpret_cast<int32_t *>(b + L.off_dw);
@@ -111,6 +119,7 @@ __device__ inline DecSmem carve_dec(uint8_t *base, const DecLayout &L, int warp)
   s.rpc = reinterpret_cast<uint32_t *>(b + L.off_rpc);
   s.win = b + L.off_win;
   s.outb = b + L.off_outb;
+  s.t01 = L.low ? b + L.off_t01 : nullptr;
   return s;
 }
 
@@ -303,7 +312,7 @@ __device__ inline void dec_unit_end(const DecSmem &s, const DecLayout &L, uint8_
 CUCM_UNROLL
   for (int o = 0; o < kOrders; o++) {
     const int n = s.ovn[o];
-    uint8_t *tb = slot + table_offset(o);
+    uint8_t *tb = (o < 2 && s.t01 ? s.t01 : slot) + table_offset(o);
     for (int e = t; e < n; e += 64) {
       const int b = s.ovl[e * kOrders + o];
       const uint32_t kk = s.ovk[o * L.NS + b];
@@ -312,8 +321,11 @@ CUCM_UNROLL
     }
   }
   const uint4 *src = reinterpret_cast<const uint4 *>(s.spl);
-  uint4 *dst = reinterpret_cast<uint4 *>(s.spf);
-  for (int i = t; i < 256 * kOrders / 4; i += 64) dst[i] = src[i];
+  uint2 *dst = reinterpret_cast<uint2 *>(s.spf);
+  for (int i = t; i < 256 * kOrders / 4; i += 64) {
+    const uint4 q = src[i];
+    dst[i] = make_uint2((q.x >> 20) | ((q.y >> 20) << 16), (q.z >> 20) | ((q.w >> 20) << 16));
+  }
   int4 *w4 = reinterpret_cast<int4 *>(s.w);
   int4 *d4 = reinterpret_cast<int4 *>(s.dw);
   for (int i = t; i < kMixCtx * kOrders / 4; i += 64) {
@@ -335,6 +347,7 @@ __device__ __forceinline__ void pair_sync(int pair) {
 }
 
 // One chunk.  role 0 decodes, role 1 updates the model; lane = threadIdx & 31.
+template <bool kLow>
 __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const DecSmem &s, const Tables *tab,
                                     const DecLayout &L, const ModelInit *init, int role, int pair,
                                     uint32_t *status) {
@@ -348,7 +361,7 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
 
   for (int i = t64; i < 256 * kOrders; i += 64) {
     const uint32_t v = init->statep[i & 7][i >> 3];
-    s.spf[i] = v;
+    s.spf[i] = (uint16_t)(v >> 20);
     s.spl[i] = v;
   }
   for (int i = t64; i < kMixCtx * kOrders; i += 64) {
@@ -356,6 +369,12 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
     s.dw[i] = 0;
   }
   for (int i = t64; i < kOrders * L.NS; i += 64) s.ovk[i] = 0;
+  if (kLow) {
+    // the chunk's order 0/1 tables move to shared memory for its lifetime
+    const uint4 *src = reinterpret_cast<const uint4 *>(slot);
+    uint4 *dst = reinterpret_cast<uint4 *>(s.t01);
+    for (int i = t64; i < (int)(kHashedOff / 16); i += 64) dst[i] = src[i];
+  }
   if (t64 < kOrders) s.ovn[t64] = 0;
   if (t64 == 0) s.prog[0] = 0;
   pair_sync(pair);
@@ -418,15 +437,19 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
       BitKeys kk;
       bit_keys64(h0, hist, kk);
       uint32_t st[kOrders];
+      if (kLow) {
+        st[0] = s.t01[kk.k[0]];
+        st[1] = s.t01[kOrder1Off + kk.k[1]];
+      }
 CUCM_UNROLL
-      for (int o = 0; o < kOrders; o++) st[o] = __ldcg(slot + table_offset(o) + kk.k[o]);
+      for (int o = kLow ? 2 : 0; o < kOrders; o++) st[o] = __ldcg(slot + table_offset(o) + kk.k[o]);
       // stretch, mixer context, mixer output (cucm_decompress_v2.cu:774-809)
       const int c1 = (int)(hist & 0xffu);
       int smp[kOrders];
       int olen = 0;
 CUCM_UNROLL
       for (int o = 0; o < kOrders; o++) {
-        smp[o] = tab->stretch[s.spf[st[o] * kOrders + o] >> 20];
+        smp[o] = tab->stretch[s.spf[st[o] * kOrders + o]];
         olen += (smp[o] != 1);
       }
       const int cxt = olen + (c1 >> 5) * 10;
@@ -500,13 +523,14 @@ CUCM_UNROLL
 
 // Grid: chunk slots in pairs of warps; warp 2c decodes chunk slot c of the
 // CTA, warp 2c + 1 updates its model.
+template <bool kLow>
 __global__ void __launch_bounds__(kDecMaxPairs * 64)
     decompress_pair_kernel(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                            const uint8_t *init_tables, const ModelInit *init, uint32_t *queue, uint32_t *status,
                            int unit) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const int pairs = blockDim.x >> 6;
-  const DecLayout L = make_dec_layout(unit, pairs);
+  const DecLayout L = make_dec_layout(unit, pairs, kLow);
   Tables *tab = reinterpret_cast<Tables *>(smem_raw + L.off_tab);
   copy_tables(&g_tables, tab);
   __syncthreads();
@@ -541,6 +565,6 @@ __global__ void __launch_bounds__(kDecMaxPairs * 64)
       pair_sync(pair);
     }
     fresh = false;
-    decompress_pair_one(t, slot, s, tab, L, init, role, pair, status);
+    decompress_pair_one<kLow>(t, slot, s, tab, L, init, role, pair, status);
   }
 }

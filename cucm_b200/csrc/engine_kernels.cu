@@ -582,7 +582,7 @@ cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *
 // Chunks (warp pairs) of the decoder that fit in one CTA's shared memory.
 static int dec_max_pairs(int unit) {
   const DecLayout one = make_dec_layout(unit, 1);
-  const size_t avail = 227 * 1024 - (one.total - one.per_warp);
+  const size_t avail = kDecSmemLimit - (one.total - one.per_warp);
   int w = (int)(avail / one.per_warp);
   return w < 1 ? 1 : (w > kDecMaxPairs ? kDecMaxPairs : w);
 }
@@ -612,12 +612,21 @@ cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t
     const int wmax = dec_max_pairs(unit);
     if (wpc > wmax) wpc = wmax;
     if (wpc < 1) wpc = 1;
-    const DecLayout L = make_dec_layout(unit, wpc);
-    cudaError_t e = set_smem((const void *)decompress_pair_kernel, L.total);
+    // up to two chunks per CTA leave room for their order 0/1 tables in
+    // shared memory
+    const DecLayout Low = make_dec_layout(unit, wpc, true);
+    const bool low = wpc <= 2 && Low.total <= kDecSmemLimit;
+    const DecLayout L = low ? Low : make_dec_layout(unit, wpc);
+    const void *kern = low ? (const void *)decompress_pair_kernel<true> : (const void *)decompress_pair_kernel<false>;
+    cudaError_t e = set_smem(kern, L.total);
     if (e != cudaSuccess) return e;
     const uint32_t grid = (nslots + (uint32_t)wpc - 1) / (uint32_t)wpc;
-    decompress_pair_kernel<<<grid, wpc * 64, L.total, stream>>>(d_tasks, ntasks, slots, nslots, init_tables, d_init,
-                                                                d_queue, d_status, unit);
+    if (low)
+      decompress_pair_kernel<true><<<grid, wpc * 64, L.total, stream>>>(d_tasks, ntasks, slots, nslots, init_tables,
+                                                                        d_init, d_queue, d_status, unit);
+    else
+      decompress_pair_kernel<false><<<grid, wpc * 64, L.total, stream>>>(d_tasks, ntasks, slots, nslots, init_tables,
+                                                                         d_init, d_queue, d_status, unit);
     return cudaGetLastError();
   }
   size_t smem = decompress_smem_bytes(unit, cfg.spec_bits);

@@ -101,3 +101,15 @@ def test_many_dev_matches_host(gpu_ctx):
                                               [(t.data_ptr(), len(b)) for t, b in zip(back, bufs)])
     assert st2 == [0] * len(bufs) and sizes2 == [len(b) for b in bufs]
     assert [bytes(t[:len(b)].cpu().numpy().tobytes()) for t, b in zip(back, bufs)] == bufs
+
+
+def test_decoder_with_many_chunks_in_flight(gpu_ctx, oracle_mod):
+    """More chunks in flight than two per SM: the decoder's CTAs then hold
+    more than two chunks each and keep the order 0/1 tables in the slot tables
+    instead of shared memory; both placements must give the same bytes."""
+    buf = W.make("text", 400 * 1024 + 123, 77).tobytes()
+    comp = gpu_ctx.compress(buf, chunksize=1024)
+    assert comp == oracle_mod.compress(buf, 1024, 128, 0, 100)
+    assert gpu_ctx.decompress(comp) == buf
+    few = buf[:2 * 1024 + 5]
+    assert gpu_ctx.decompress(gpu_ctx.compress(few, chunksize=1024)) == few
