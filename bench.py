@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="mixed256M", choices=["mixed256M", "batch", "serve", "small"])
+    ap.add_argument("--autotune", action="store_true",
+                    help="mixed256M: choose the execution form with the measured autotuner first (untimed, on a "
+                         "32 MiB sample cut into the same 256 chunks)")
     ap.add_argument("--plain-sample", type=int, default=512, help="buffers the plain form codes (batch)")
     ap.add_argument("--requests", type=int, default=48, help="requests per offered load (serve)")
     ap.add_argument("--loads", default="0.02,0.2,2,8,32", help="offered loads in GB/s (serve)")
@@ -296,6 +299,16 @@ def main():
     n = data.size
     form = cc.FORM_PLAIN if args.form == "plain" else cc.FORM_PERSISTENT
     ctx = cc.Context(local, form=form)
+    tuned = None
+    if args.autotune:
+        nch = n // PARAMS["chunksize"]
+        sample = data[:32 << 20]
+        best, cands = ctx.autotune(sample, reps=1, chunksize=max(sample.size // max(nch, 1), 4096),
+                                   unit=PARAMS["unit"], batch=PARAMS["batch"])
+        tuned = {"chosen": {k: best[k] for k in ("form", "dec_pairs", "dec_tables")},
+                 "sample": "first 32 MiB, %d chunks" % nch,
+                 "candidates": [{k: c[k] for k in ("form", "dec_pairs", "dec_tables", "compress_ms",
+                                                   "decompress_ms")} for c in cands]}
     p = cc.default_params(**PARAMS)
     cap = cc.lib().cucm_compress_bound(n, p)
     d_in = torch.from_numpy(data).to(dev)
@@ -401,13 +414,16 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": "mixed 256 MiB per rank, 1 MiB chunks (256), unit 128, batch 100",
                    "form": args.form, "chunksize": PARAMS["chunksize"], "unit": 128, "batch": 100,
-                   "parallelism": "independent chunks per rank", "l2": "inputs larger than L2"},
+                   "parallelism": "independent chunks per rank", "l2": "inputs larger than L2",
+                   "tuning": ctx.get_tuning()},
         "compress_MBps": world * n * K / (t_c / 1e3) / 1e6, "decompress_MBps": world * n * K / (t_d / 1e3) / 1e6,
         "compressed_bytes": int(comp_n), "ratio": n / comp_n,
         "kernel_ms": {"compress": kc / K, "decompress": kd / K},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": launches,
     }
+    if tuned:
+        line["autotune"] = tuned
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

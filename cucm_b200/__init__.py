@@ -23,12 +23,12 @@ LIB_PATH = os.path.join(_PKG, "libcucm.so")
 FORM_AUTO, FORM_PLAIN, FORM_PERSISTENT = 0, 1, 2
 
 CUCM_OK = 0
-EINVAL, ENOSPC, EFORMAT = -1, -2, -3
+EINVAL, ENOSPC, EFORMAT, EMISMATCH = -1, -2, -3, -10
 PENDING = 1
 OP_COMPRESS, OP_DECOMPRESS = 0, 1
 _ERRORS = {
     -1: "EINVAL", -2: "ENOSPC", -3: "EFORMAT", -4: "ENOMEM", -5: "ECUDA",
-    -6: "ENODEV", -7: "ETIMEOUT", -8: "EBUSY", -9: "ENOTFOUND",
+    -6: "ENODEV", -7: "ETIMEOUT", -8: "EBUSY", -9: "ENOTFOUND", -10: "EMISMATCH",
 }
 
 
@@ -57,7 +57,16 @@ class ServerInfo(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("spec_bits", ctypes.c_int),
-                ("max_slots", ctypes.c_int), ("hbm_budget", ctypes.c_uint64), ("kernel", ctypes.c_int)]
+                ("max_slots", ctypes.c_int), ("hbm_budget", ctypes.c_uint64), ("kernel", ctypes.c_int),
+                ("dec_pairs", ctypes.c_int), ("dec_tables", ctypes.c_int), ("cmp_ctas", ctypes.c_int)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("tuning", Tuning), ("compress_ms", ctypes.c_double), ("decompress_ms", ctypes.c_double)]
+
+
+def _tuning_dict(t):
+    return {f: getattr(t, f) for f, _ in Tuning._fields_}
 
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
@@ -71,6 +80,10 @@ SIGNATURES = [
     ("cucm_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_void_p)]),
     ("cucm_ctx_destroy", ctypes.c_int, [ctypes.c_void_p]),
     ("cucm_ctx_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    ("cucm_ctx_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    ("cucm_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Params),
+                                     ctypes.c_int, ctypes.POINTER(TuneResult), ctypes.c_uint32,
+                                     ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(Tuning)]),
     ("cucm_compress_bound", ctypes.c_uint64, [ctypes.c_uint64, ctypes.POINTER(Params)]),
     ("cucm_decompressed_size", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _u64p]),
     ("cucm_compress", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Params),
@@ -175,9 +188,10 @@ def _buf(data):
 class Context:
     """One CUDA device, one stream and the device pools of the coder."""
 
-    def __init__(self, device=0, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0):
+    def __init__(self, device=0, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0, dec_pairs=0,
+                 dec_tables=0, cmp_ctas=0):
         self._h = ctypes.c_void_p()
-        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel)
+        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas)
         rc = lib().cucm_ctx_create(int(device), ctypes.byref(t), ctypes.byref(self._h))
         if rc:
             raise CucmError(rc, "cucm_ctx_create")
@@ -199,11 +213,35 @@ class Context:
         except Exception:
             pass
 
-    def set_tuning(self, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0):
-        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel)
+    def set_tuning(self, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0, dec_pairs=0, dec_tables=0,
+                   cmp_ctas=0):
+        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas)
         rc = lib().cucm_ctx_set_tuning(self._h, ctypes.byref(t))
         if rc:
             raise CucmError(rc, "cucm_ctx_set_tuning")
+
+    def get_tuning(self):
+        t = Tuning()
+        rc = lib().cucm_ctx_get_tuning(self._h, ctypes.byref(t))
+        if rc:
+            raise CucmError(rc, "cucm_ctx_get_tuning")
+        return _tuning_dict(t)
+
+    def autotune(self, sample, reps=1, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+        """Measure every execution choice on `sample` (cucm_autotune), apply
+        the fastest and return (chosen tuning, [measured candidates])."""
+        p = default_params(chunksize, unit, prelearn, batch)
+        ptr, n, keep = _buf(sample)
+        res = (TuneResult * 64)()
+        count = ctypes.c_uint32()
+        best = Tuning()
+        rc = lib().cucm_autotune(self._h, ptr, n, ctypes.byref(p), int(reps), res, 64, ctypes.byref(count),
+                                 ctypes.byref(best))
+        if rc:
+            raise CucmError(rc, "cucm_autotune")
+        cands = [dict(_tuning_dict(r.tuning), compress_ms=r.compress_ms, decompress_ms=r.decompress_ms)
+                 for r in res[:min(count.value, 64)]]
+        return _tuning_dict(best), cands
 
     def compress(self, data, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
         p = default_params(chunksize, unit, prelearn, batch)
@@ -415,7 +453,7 @@ class Server:
 
     def __init__(self, device=0, hbm_budget=0, max_slots=0, kernel=0):
         self._h = ctypes.c_void_p()
-        t = Tuning(FORM_PERSISTENT, 0, max_slots, hbm_budget, kernel)
+        t = Tuning(FORM_PERSISTENT, 0, max_slots, hbm_budget, kernel, 0, 0, 0)
         rc = lib().cucm_server_create(device, hbm_budget, ctypes.byref(t), ctypes.byref(self._h))
         if rc:
             raise CucmError(rc, "cucm_server_create")

@@ -25,7 +25,7 @@ WORKLOAD_LIB = os.path.join(PKG, "libcucm_workload.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
            "-I" + os.path.join(ROOT, "include")]
-CU_SOURCES = ["engine_kernels.cu", "api.cu", "serve.cu", "noalloc.cu"]
+CU_SOURCES = ["engine_kernels.cu", "api.cu", "serve.cu", "noalloc.cu", "autotune.cu"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
 
 

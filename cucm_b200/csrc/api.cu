@@ -171,6 +171,9 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
   cfg.spec_bits = c->tuning.spec_bits > 0 ? c->tuning.spec_bits : 4;
   cfg.generic = c->tuning.kernel == 1;
   cfg.sm_count = c->sm_count;
+  cfg.dec_pairs = c->tuning.dec_pairs;
+  cfg.dec_tables = c->tuning.dec_tables;
+  cfg.cmp_ctas = c->tuning.cmp_ctas;
   const int form = c->tuning.form == CUCM_FORM_PLAIN ? CUCM_FORM_PLAIN : CUCM_FORM_PERSISTENT;
 
   int rc = upload_model(c, ms);
@@ -423,6 +426,7 @@ const char *cucm_strerror(int s) {
     case CUCM_ETIMEOUT: return "bounded device wait expired";
     case CUCM_EBUSY: return "serving queue full";
     case CUCM_ENOTFOUND: return "unknown request";
+    case CUCM_EMISMATCH: return "execution choices gave different bytes";
     default: return "unknown error";
   }
 }
@@ -474,6 +478,13 @@ int cucm_ctx_set_tuning(cucm_ctx *c, const cucm_tuning *t) {
   if (!c || !t) return CUCM_EINVAL;
   std::lock_guard<std::mutex> g(c->mu);
   c->tuning = *t;
+  return CUCM_OK;
+}
+
+int cucm_ctx_get_tuning(cucm_ctx *c, cucm_tuning *t) {
+  if (!c || !t) return CUCM_EINVAL;
+  std::lock_guard<std::mutex> g(c->mu);
+  *t = c->tuning;
   return CUCM_OK;
 }
 

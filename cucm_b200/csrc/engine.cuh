@@ -41,6 +41,9 @@ struct EngineConfig {
   int spec_bits = 4;           // decoder speculation depth (1..8); never changes output
   bool generic = false;        // force the generic (non-pipelined) kernels
   int sm_count = 0;            // SMs of the device (0 = query)
+  int dec_pairs = 0;           // decoder chunks per CTA (0 = spread over all SMs first)
+  int dec_tables = 0;          // decoder order 0/1 tables: 0 = shared memory where it fits, 1 = slot tables
+  int cmp_ctas = 0;            // pipelined compressor CTAs per SM (0 = derived)
 };
 
 cudaError_t upload_tables();  // once per device (current device)

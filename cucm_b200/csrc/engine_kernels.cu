@@ -19,6 +19,7 @@
 //
 // A CTA takes chunks from a global queue (persistent form) until it is
 // empty; the plain form launches one single-CTA grid per chunk.
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -590,8 +591,9 @@ static int dec_max_pairs(int unit) {
 static bool dec_fast(int unit, const EngineConfig &cfg) { return unit <= kDecMaxUnit && !cfg.generic; }
 
 int engine_slots_per_sm(bool decode, int unit, const EngineConfig &cfg) {
-  if (decode && dec_fast(unit, cfg)) return dec_max_pairs(unit);
-  if (!decode && unit <= kFastMaxUnit && !cfg.generic) return 2;
+  if (decode && dec_fast(unit, cfg))
+    return cfg.dec_pairs > 0 ? std::min(cfg.dec_pairs, dec_max_pairs(unit)) : dec_max_pairs(unit);
+  if (!decode && unit <= kFastMaxUnit && !cfg.generic) return cfg.cmp_ctas == 1 ? 1 : 2;
   const size_t smem = decode ? decompress_smem_bytes(unit, cfg.spec_bits) : make_layout(unit, 0).total;
   return smem > 110 * 1024 ? 1 : (smem > 72 * 1024 ? 2 : 3);
 }
@@ -610,12 +612,13 @@ cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t
     }
     int wpc = (int)((nslots + (uint32_t)sms - 1) / (uint32_t)sms);
     const int wmax = dec_max_pairs(unit);
+    if (cfg.dec_pairs > 0) wpc = cfg.dec_pairs;
     if (wpc > wmax) wpc = wmax;
     if (wpc < 1) wpc = 1;
     // up to two chunks per CTA leave room for their order 0/1 tables in
     // shared memory
     const DecLayout Low = make_dec_layout(unit, wpc, true);
-    const bool low = wpc <= 2 && Low.total <= kDecSmemLimit;
+    const bool low = cfg.dec_tables == 0 && wpc <= 2 && Low.total <= kDecSmemLimit;
     const DecLayout L = low ? Low : make_dec_layout(unit, wpc);
     const void *kern = low ? (const void *)decompress_pair_kernel<true> : (const void *)decompress_pair_kernel<false>;
     cudaError_t e = set_smem(kern, L.total);

@@ -277,6 +277,9 @@ int run_tasks(cucm_server *s, Launch *l, const std::vector<ChunkTask> &tasks) {
   cfg.spec_bits = s->tuning.spec_bits > 0 ? s->tuning.spec_bits : 4;
   cfg.generic = s->tuning.kernel == 1;
   cfg.sm_count = s->sm_count;
+  cfg.dec_pairs = s->tuning.dec_pairs;
+  cfg.dec_tables = s->tuning.dec_tables;
+  cfg.cmp_ctas = s->tuning.cmp_ctas;
   std::vector<ChunkTask> order = tasks;
   const bool dec = l->op == CUCM_OP_DECOMPRESS;
   std::stable_sort(order.begin(), order.end(), [&](const ChunkTask &a, const ChunkTask &b) {

@@ -41,6 +41,7 @@ extern "C" {
 #define CUCM_ETIMEOUT (-7)   /* a bounded device wait expired */
 #define CUCM_EBUSY (-8)      /* serving queue full */
 #define CUCM_ENOTFOUND (-9)  /* unknown request id */
+#define CUCM_EMISMATCH (-10) /* autotuner: two execution choices gave different bytes */
 
 /* Stream parameters: the reference's CLI flags -s -u -p -b
  * (cucm_compress_v2.cu:1288-1299).  They are stored in the container header
@@ -65,6 +66,9 @@ typedef struct cucm_tuning {
   int max_slots;       /* cap on resident chunk slots (0 = derive from budget) */
   uint64_t hbm_budget; /* device bytes this context may hold (0 = 90% of free) */
   int kernel;          /* 0 = pipelined kernels where the unit allows, 1 = generic kernels */
+  int dec_pairs;       /* decoder chunks (warp pairs) per CTA, 0 = spread over all SMs first */
+  int dec_tables;      /* decoder order 0/1 tables: 0 = shared memory where it fits, 1 = slot tables */
+  int cmp_ctas;        /* pipelined compressor CTAs (chunks) per SM, 1 or 2; 0 = derived */
 } cucm_tuning;
 
 typedef struct cucm_ctx cucm_ctx;
@@ -77,6 +81,7 @@ const char *cucm_version(void);
 int cucm_ctx_create(int device, const cucm_tuning *tuning, cucm_ctx **out);
 int cucm_ctx_destroy(cucm_ctx *ctx);
 int cucm_ctx_set_tuning(cucm_ctx *ctx, const cucm_tuning *tuning);
+int cucm_ctx_get_tuning(cucm_ctx *ctx, cucm_tuning *tuning);
 
 /* Largest container cucm_compress can produce for n input bytes. */
 uint64_t cucm_compress_bound(uint64_t n, const cucm_params *p);
@@ -183,6 +188,26 @@ int cucm_last_launches(cucm_ctx *ctx, uint64_t *n);
 /* Figures of the last call: device_ms as above, kernel_ms the time of the
  * coder kernels alone (CUDA events around their launches), launches, and
  * the number of chunks coded. */
+/* Measured autotuner.  No counterpart in the reference, whose launch
+ * shapes are fixed.  Codes `sample` (host memory, n bytes) with `p` under
+ * every candidate execution choice -- launch form; for the persistent
+ * compressor, CTAs per SM (1, 2); for the persistent decoder, chunks per
+ * CTA (0..5) and order 0/1 table placement -- `reps`
+ * times each (>= 1; the fastest repetition counts), checks that every
+ * candidate gives the same container and gives the sample back (else
+ * CUCM_EMISMATCH), then applies to the context and writes to *best the
+ * choice with the least compress + decompress device time.  The other
+ * tuning fields are kept.  results (may be null) receives up to `cap`
+ * measured candidates, *count their number.  A sample with the target
+ * workload's number of chunks gives choices that carry over to it. */
+typedef struct cucm_tune_result {
+  cucm_tuning tuning;
+  double compress_ms;   /* fastest compress of the sample (< 0: a decoder candidate) */
+  double decompress_ms; /* fastest decompress of the sample (< 0: a compressor candidate) */
+} cucm_tune_result;
+int cucm_autotune(cucm_ctx *ctx, const uint8_t *sample, uint64_t n, const cucm_params *p, int reps,
+                  cucm_tune_result *results, uint32_t cap, uint32_t *count, cucm_tuning *best);
+
 typedef struct cucm_stats {
   double device_ms;
   double kernel_ms;

@@ -72,5 +72,20 @@ def test_compress_bound_and_size_query(cucm_lib):
 
 
 def test_strerror(cucm_lib):
-    for s in range(0, -10, -1):
+    for s in range(0, -11, -1):
         assert cucm_lib.cucm_strerror(s)
+    assert b"different bytes" in cucm_lib.cucm_strerror(cucm_b200.EMISMATCH)
+
+
+def test_tuning_layout_and_autotune_arguments(cucm_lib):
+    # cucm_tuning: form, spec_bits, max_slots, (pad), hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas
+    assert ctypes.sizeof(cucm_b200.Tuning) == 40
+    assert (cucm_b200.Tuning.dec_tables.offset, cucm_b200.Tuning.cmp_ctas.offset) == (32, 36)
+    assert cucm_lib.cucm_ctx_get_tuning(None, None) == -1
+    t = cucm_b200.Tuning()
+    p = cucm_b200.default_params()
+    n = ctypes.c_uint32()
+    buf = ctypes.create_string_buffer(16)
+    assert cucm_lib.cucm_autotune(None, buf, 16, ctypes.byref(p), 1, None, 0, ctypes.byref(n), ctypes.byref(t)) == -1
+    # a null result array with a nonzero capacity is refused before any device work
+    assert cucm_lib.cucm_autotune(None, buf, 16, ctypes.byref(p), 1, None, 4, ctypes.byref(n), ctypes.byref(t)) == -1
