@@ -62,7 +62,7 @@ __host__ __device__ inline DecLayout make_dec_layout(int U, int warps, bool low 
     o = (o + bytes + 15) & ~(size_t)15;
     return at;
   };
-  L.off_spf = take(sizeof(uint16_t) * 256 * kOrders);          // frozen probability (statep >> 20) [state][order]
+  L.off_spf = take(sizeof(int16_t) * 256 * kOrders);           // frozen probability, stretched [state][order]
   L.off_spl = take(sizeof(uint32_t) * 256 * kOrders);          // live statep [state][order]
   L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);         // frozen weights
   L.off_dw = take(sizeof(int32_t) * kMixCtx * kOrders);        // summed deltas of the unit
@@ -85,7 +85,7 @@ __host__ __device__ inline DecLayout make_dec_layout(int U, int warps, bool low 
 }
 
 struct DecSmem {
-  uint16_t *spf;
+  int16_t *spf;
   uint32_t *spl;
   int32_t *w, *dw;
   uint32_t *ovk;
@@ -104,7 +104,7 @@ struct DecSmem {
 __device__ inline DecSmem carve_dec(uint8_t *base, const DecLayout &L, int warp) {
   uint8_t *b = base + (size_t)warp * L.per_warp;
   DecSmem s;
-  s.spf = reinterpret_cast<uint16_t *>(b + L.off_spf);
+  s.spf = reinterpret_cast<int16_t *>(b + L.off_spf);
   s.spl = reinterpret_cast<uint32_t *>(b + L.off_spl);
   s.w = reinterpret_cast<int32_t *>(b + L.off_w);
   s.dw = reinterpret_cast<int32_t *>(b + L.off_dw);
@@ -305,10 +305,11 @@ CUCM_UNROLL
 }
 
 // Unit end, both warps of the pair (t = 0..63): overlay -> slot tables (and
-// cleared), live probabilities become frozen, deltas join the weights, the
-// unit's bytes go out.  Called between two pair barriers.
-__device__ inline void dec_unit_end(const DecSmem &s, const DecLayout &L, uint8_t *slot, uint8_t *out, int nbytes,
-                                    int t) {
+// cleared), live probabilities become frozen (stretched for the mixer),
+// deltas join the weights, the unit's bytes go out.  Called between two pair
+// barriers.
+__device__ inline void dec_unit_end(const DecSmem &s, const DecLayout &L, const Tables *tab, uint8_t *slot,
+                                    uint8_t *out, int nbytes, int t) {
 CUCM_UNROLL
   for (int o = 0; o < kOrders; o++) {
     const int n = s.ovn[o];
@@ -322,9 +323,13 @@ CUCM_UNROLL
   }
   const uint4 *src = reinterpret_cast<const uint4 *>(s.spl);
   uint2 *dst = reinterpret_cast<uint2 *>(s.spf);
+  const int16_t *str = tab->stretch;
+#pragma unroll 4
   for (int i = t; i < 256 * kOrders / 4; i += 64) {
     const uint4 q = src[i];
-    dst[i] = make_uint2((q.x >> 20) | ((q.y >> 20) << 16), (q.z >> 20) | ((q.w >> 20) << 16));
+    const uint32_t a = (uint16_t)str[q.x >> 20], b = (uint16_t)str[q.y >> 20];
+    const uint32_t c = (uint16_t)str[q.z >> 20], d = (uint16_t)str[q.w >> 20];
+    dst[i] = make_uint2(a | (b << 16), c | (d << 16));
   }
   int4 *w4 = reinterpret_cast<int4 *>(s.w);
   int4 *d4 = reinterpret_cast<int4 *>(s.dw);
@@ -361,7 +366,7 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
 
   for (int i = t64; i < 256 * kOrders; i += 64) {
     const uint32_t v = init->statep[i & 7][i >> 3];
-    s.spf[i] = (uint16_t)(v >> 20);
+    s.spf[i] = tab->stretch[v >> 20];
     s.spl[i] = v;
   }
   for (int i = t64; i < kMixCtx * kOrders; i += 64) {
@@ -401,7 +406,7 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
       if (lane < kOrders) s.ovn[lane] = nov;
       if (!ok && lane == 0) atomicOr(status, (uint32_t)kDevTimeout);
       pair_sync(pair);
-      dec_unit_end(s, L, slot, t.out + (base >> 3), nunit >> 3, t64);
+      dec_unit_end(s, L, tab, slot, t.out + (base >> 3), nunit >> 3, t64);
       pair_sync(pair);
     }
     return;
@@ -449,7 +454,7 @@ CUCM_UNROLL
       int olen = 0;
 CUCM_UNROLL
       for (int o = 0; o < kOrders; o++) {
-        smp[o] = tab->stretch[s.spf[st[o] * kOrders + o]];
+        smp[o] = s.spf[st[o] * kOrders + o];
         olen += (smp[o] != 1);
       }
       const int cxt = olen + (c1 >> 5) * 10;
@@ -516,7 +521,7 @@ CUCM_UNROLL
       }
     }
     pair_sync(pair);
-    dec_unit_end(s, L, slot, t.out + (base >> 3), nunit >> 3, t64);
+    dec_unit_end(s, L, tab, slot, t.out + (base >> 3), nunit >> 3, t64);
     pair_sync(pair);
   }
 }
