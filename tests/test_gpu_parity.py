@@ -36,13 +36,13 @@ def test_golden_compress(gpu_ctx, entry, form):
     assert got == golden
 
 
-# decoders: the one-warp kernel (units <= 256), and the generic kernel at
+# decoders: the warp-pair kernel (units <= 256), and the generic kernel at
 # three speculation depths
 DECODERS = [(0, 0), (1, 1), (1, 4), (1, 8)]
 
 
 @pytest.mark.parametrize("entry", MANIFEST, ids=lambda e: e["name"])
-@pytest.mark.parametrize("kernel,spec", DECODERS, ids=["warp", "generic1", "generic4", "generic8"])
+@pytest.mark.parametrize("kernel,spec", DECODERS, ids=["pair", "generic1", "generic4", "generic8"])
 def test_golden_decompress(gpu_ctx, entry, kernel, spec):
     gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT, spec_bits=spec, kernel=kernel)
     with open(os.path.join(GOLDEN, entry["name"] + ".cucm"), "rb") as f:
