@@ -10,22 +10,24 @@
 // The decoding warp:
 //   * gives the 15 nodes of the nibble's speculation tree (every prefix of
 //     0..3 bits) their 8 context keys and frozen slot states -- one lane per
-//     node, 8 gathers in flight per lane, so a round costs one memory round
-//     trip;
-//   * stretches, mixes and squashes each node's prediction against the
-//     frozen model and decodes the 4 bits uniformly (every lane runs the same
-//     coder arithmetic; the split point of a node comes from its lane by
-//     shuffle);
+//     node, its 6 hashed orders' gathers in flight together (orders 0 and 1
+//     come from shared memory when the CTA has room for them), so a round
+//     costs one memory round trip;
+//   * mixes and squashes each node's prediction against the frozen model
+//     (probabilities kept stretched) and decodes the 4 bits uniformly (every
+//     lane runs the same coder arithmetic; the split point of a node comes
+//     from its lane by shuffle);
 //   * has the 4 lanes on the decoded path record keys, states and mixer
 //     inputs of their bit in a per-unit ring, and publishes the round.
-// The updating warp follows one round behind (lane = order): the bit-history
-// walk through a per-unit overlay (slot -> live state), the StateMap
-// probability chain and the mixer deltas, all in bit order.  Nothing the
-// decoding warp reads changes before the unit ends, so the two only meet
-// there: the overlay's states go to the slot tables, the live probabilities
-// become the frozen ones and the summed mixer deltas join the weights
-// (updateStateMap / updateMixer, cucm_decompress_v2.cu:870-896).  Rounds
-// never straddle a unit or byte boundary: units are multiples of 32 bits.
+// The updating warp follows one round behind (lane = order), polling for
+// published rounds: the bit-history walk through a per-unit overlay (slot ->
+// live state, 4-key buckets), the StateMap probability chain and the mixer
+// deltas, all in bit order.  Nothing the decoding warp reads changes before
+// the unit ends, so the two only meet there: the overlay's states go to the
+// slot tables, the live probabilities become the frozen ones and the summed
+// mixer deltas join the weights (updateStateMap / updateMixer,
+// cucm_decompress_v2.cu:870-896).  Rounds never straddle a unit or byte
+// boundary: units are multiples of 32 bits.
 //
 // Several warp pairs of a CTA decode independent chunks and share the
 // read-only tables.
