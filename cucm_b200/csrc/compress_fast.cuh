@@ -10,20 +10,21 @@
 //   front warps (3..6, 128 threads)
 //     * keys of unit t+2 for all 8 orders (one FNV pass per bit,
 //       cucm_compress_v2.cu:723-747), the unit's bits and previous bytes;
-//     * slot links of unit t+1: a shared-memory hash table per order maps
-//       each slot of the unit to a bucket; atomicMin on the bucket gives the
-//       first touch in bit order, so every later touch knows it must read the
-//       state its predecessor left; a probe of the previous unit's table
+//     * slot links of unit t+1: a shared-memory hash table per order (4-key
+//       buckets, places claimed by warp match and rank) gives every distinct
+//       slot of the unit one place, so every later touch knows it must read
+//       the state its predecessor left; a probe of the previous unit's table
 //       tells whether the slot was touched one unit earlier;
 //     * gathers of unit t+1's slot states from the tables in HBM;
 //     * stretch, mixer context, mixer output and training of unit t-1
 //       (cudamixUnit / cudaupdateMixer, cucm_compress_v2.cu:755-819) against
 //       a snapshot of the probabilities taken when the previous chain ended.
-//   walker warp (2, lane = order): the bit-history side of the StateMap
-//     update for unit t, in bit order: the state each update sees (live), the
-//     state each prediction saw (frozen = unit-start value), the next state,
-//     written through to the slot table.  It only depends on the bits, never
-//     on the probabilities, so it runs a unit ahead of the chain.
+//   walker warp (2): the bit-history side of the StateMap update for unit
+//     t, in bit order, a byte (64 updates) per step: the state each update
+//     sees (live), the state each prediction saw (frozen = unit-start value),
+//     the next state, written through to the slot table.  It only depends on
+//     the bits, never on the probabilities, so it runs a unit ahead of the
+//     chain.
 //   chain warp (0, lane = order): the StateMap probability updates of unit
 //     t-1 in bit order (cucm_compress_v2.cu:592-601); the adaptation rate is
 //     carried next to each probability.
@@ -181,26 +182,7 @@ __device__ __forceinline__ void front_keys(const FastSmem &s, const FastLayout &
 
 // Slot tables: per order, NSLOT/4 buckets of 4 keys (key + 1, 0 = empty),
 // probed with one 16-byte load per bucket; a full bucket spills to the next.
-__device__ __forceinline__ int slot_insert(uint32_t *row, int logNBK, uint32_t kp) {
-  const uint32_t nbk_mask = (1u << logNBK) - 1u;
-  uint32_t b = bucket_of(kp - 1, logNBK);
-  for (;;) {
-    const uint4 q = *reinterpret_cast<const uint4 *>(row + 4 * b);
-    if (q.x == kp) return 4 * b;
-    if (q.y == kp) return 4 * b + 1;
-    if (q.z == kp) return 4 * b + 2;
-    if (q.w == kp) return 4 * b + 3;
-    const int e = q.x == 0 ? 0 : (q.y == 0 ? 1 : (q.z == 0 ? 2 : (q.w == 0 ? 3 : -1)));
-    if (e < 0) {
-      b = (b + 1) & nbk_mask;
-      continue;
-    }
-    const uint32_t old = atomicCAS(row + 4 * b + e, 0u, kp);
-    if (old == 0 || old == kp) return 4 * b + e;
-    // another key took the slot: look at the bucket again
-  }
-}
-
+// Slot of key kp (key + 1) in a table, or -1.
 __device__ __forceinline__ int slot_find(const uint32_t *row, int logNBK, uint32_t kp) {
   const uint32_t nbk_mask = (1u << logNBK) - 1u;
   uint32_t b = bucket_of(kp - 1, logNBK);
