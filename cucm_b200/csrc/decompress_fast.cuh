@@ -36,7 +36,6 @@ constexpr int kDecMaxUnit = 256;
 constexpr int kDecMaxPairs = 8;          // chunks per CTA
 constexpr int kDecWin = 2048;            // payload window per chunk (bytes)
 constexpr int kDecNodes = 15;            // nodes of a 4-bit speculation tree
-constexpr int kDecRecBytes = 240;        // one round's records
 constexpr size_t kDecSmemLimit = 227 * 1024;  // dynamic shared memory of one CTA
 constexpr uint32_t kDecSpinLimit = 1u << 27;  // polls bounding the updater's wait for a round (seconds)
 
