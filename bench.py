@@ -101,6 +101,18 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def reference_sha256(key):
+    """SHA-256 of the reference's container for a full-size workload, from the
+    committed manifest (tests/golden/fullsize_manifest.json, written by the
+    reference's own compressor), or None."""
+    p = os.path.join(ROOT, "tests", "golden", "fullsize_manifest.json")
+    try:
+        with open(p) as f:
+            return json.load(f)[key]["output_sha256"]
+    except Exception:
+        return None
+
+
 def profile_traffic():
     """DRAM bytes per full-size launch of each kernel, from the committed ncu
     summary (profiles/traffic_mixed256M.json), if present."""
@@ -327,6 +339,10 @@ def main():
         comp_n, _, _ = step()
     if not torch.equal(d_dec, d_in):
         raise SystemExit("round trip mismatch on the device")
+    # the container of the timed workload against the reference's (by hash)
+    import hashlib
+    got_sha = hashlib.sha256(d_comp[:comp_n].cpu().numpy().tobytes()).hexdigest() if args.warmup > 0 else None
+    want_sha = reference_sha256("mixed256M")
 
     def barrier():
         if dist is not None:
@@ -418,6 +434,8 @@ def main():
                    "tuning": ctx.get_tuning()},
         "compress_MBps": world * n * K / (t_c / 1e3) / 1e6, "decompress_MBps": world * n * K / (t_d / 1e3) / 1e6,
         "compressed_bytes": int(comp_n), "ratio": n / comp_n,
+        "sha256_match": (got_sha == want_sha) if (got_sha and want_sha) else None,
+        "sha256_reference": "container of the reference's own compressor (tests/golden/fullsize_manifest.json)",
         "kernel_ms": {"compress": kc / K, "decompress": kd / K},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": launches,

@@ -58,7 +58,14 @@ class ServerInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("spec_bits", ctypes.c_int),
                 ("max_slots", ctypes.c_int), ("hbm_budget", ctypes.c_uint64), ("kernel", ctypes.c_int),
-                ("dec_pairs", ctypes.c_int), ("dec_tables", ctypes.c_int), ("cmp_ctas", ctypes.c_int)]
+                ("dec_pairs", ctypes.c_int), ("dec_tables", ctypes.c_int), ("cmp_ctas", ctypes.c_int),
+                ("dec_spin_limit", ctypes.c_uint32)]
+
+
+def make_tuning(form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0, dec_pairs=0, dec_tables=0,
+                cmp_ctas=0, dec_spin_limit=0):
+    """A cucm_tuning; 0 everywhere means the derived defaults."""
+    return Tuning(form, spec_bits, max_slots, hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas, dec_spin_limit)
 
 
 class TuneResult(ctypes.Structure):
@@ -118,6 +125,7 @@ SIGNATURES = [
     ("cucm_serve_poll", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                        _u64p, ctypes.POINTER(ctypes.c_double)]),
     ("cucm_server_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerInfo)]),
+    ("cucm_server_set_queue_limit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     ("cucm_last_device_ms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ("cucm_last_launches", ctypes.c_int, [ctypes.c_void_p, _u64p]),
     ("cucm_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
@@ -188,10 +196,9 @@ def _buf(data):
 class Context:
     """One CUDA device, one stream and the device pools of the coder."""
 
-    def __init__(self, device=0, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0, dec_pairs=0,
-                 dec_tables=0, cmp_ctas=0):
+    def __init__(self, device=0, **tuning):
         self._h = ctypes.c_void_p()
-        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas)
+        t = make_tuning(**tuning)
         rc = lib().cucm_ctx_create(int(device), ctypes.byref(t), ctypes.byref(self._h))
         if rc:
             raise CucmError(rc, "cucm_ctx_create")
@@ -213,9 +220,9 @@ class Context:
         except Exception:
             pass
 
-    def set_tuning(self, form=FORM_AUTO, spec_bits=0, max_slots=0, hbm_budget=0, kernel=0, dec_pairs=0, dec_tables=0,
-                   cmp_ctas=0):
-        t = Tuning(form, spec_bits, max_slots, hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas)
+    def set_tuning(self, **tuning):
+        """Replace the execution choices (make_tuning's keywords; omitted = 0)."""
+        t = make_tuning(**tuning)
         rc = lib().cucm_ctx_set_tuning(self._h, ctypes.byref(t))
         if rc:
             raise CucmError(rc, "cucm_ctx_set_tuning")
@@ -453,7 +460,7 @@ class Server:
 
     def __init__(self, device=0, hbm_budget=0, max_slots=0, kernel=0):
         self._h = ctypes.c_void_p()
-        t = Tuning(FORM_PERSISTENT, 0, max_slots, hbm_budget, kernel, 0, 0, 0)
+        t = make_tuning(form=FORM_PERSISTENT, max_slots=max_slots, hbm_budget=hbm_budget, kernel=kernel)
         rc = lib().cucm_server_create(device, hbm_budget, ctypes.byref(t), ctypes.byref(self._h))
         if rc:
             raise CucmError(rc, "cucm_server_create")
@@ -508,6 +515,11 @@ class Server:
         keep, out, optr = self._live.pop(rid)
         data = ctypes.string_at(optr, n.value) if st.value == 0 else None
         return st.value, data, lat.value
+
+    def set_queue_limit(self, limit):
+        rc = lib().cucm_server_set_queue_limit(self._h, int(limit))
+        if rc:
+            raise CucmError(rc, "cucm_server_set_queue_limit")
 
     def stats(self):
         info = ServerInfo()

@@ -174,6 +174,7 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
   cfg.dec_pairs = c->tuning.dec_pairs;
   cfg.dec_tables = c->tuning.dec_tables;
   cfg.cmp_ctas = c->tuning.cmp_ctas;
+  cfg.spin_limit = c->tuning.dec_spin_limit;
   const int form = c->tuning.form == CUCM_FORM_PLAIN ? CUCM_FORM_PLAIN : CUCM_FORM_PERSISTENT;
 
   int rc = upload_model(c, ms);

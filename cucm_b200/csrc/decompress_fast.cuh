@@ -37,7 +37,7 @@ constexpr int kDecMaxPairs = 8;          // chunks per CTA
 constexpr int kDecWin = 2048;            // payload window per chunk (bytes)
 constexpr int kDecNodes = 15;            // nodes of a 4-bit speculation tree
 constexpr size_t kDecSmemLimit = 227 * 1024;  // dynamic shared memory of one CTA
-constexpr uint32_t kDecSpinLimit = 1u << 27;  // polls bounding the updater's wait for a round (seconds)
+constexpr uint32_t kDecSpinLimit = 1u << 27;  // default bound on the updater's polls for a round (seconds)
 
 struct DecLayout {
   int U, NS, logNS, warps, rounds;
@@ -356,7 +356,7 @@ __device__ __forceinline__ void pair_sync(int pair) {
 template <bool kLow>
 __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const DecSmem &s, const Tables *tab,
                                     const DecLayout &L, const ModelInit *init, int role, int pair,
-                                    uint32_t *status) {
+                                    uint32_t *status, uint32_t spin_limit) {
   const int lane = threadIdx.x & 31;
   const int t64 = lane + 32 * role;
   const int U = L.U;
@@ -397,7 +397,7 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
         while (ok && s.prog[0] <= done) {
           // a plain poll: a sleep here wakes late and the updating warp
           // falls rounds behind by the unit's end
-          if (++spins >= kDecSpinLimit) ok = false;
+          if (++spins >= spin_limit) ok = false;
         }
         __threadfence_block();
         if (!ok) break;
@@ -533,7 +533,7 @@ template <bool kLow>
 __global__ void __launch_bounds__(kDecMaxPairs * 64)
     decompress_pair_kernel(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                            const uint8_t *init_tables, const ModelInit *init, uint32_t *queue, uint32_t *status,
-                           int unit) {
+                           int unit, uint32_t spin_limit) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const int pairs = blockDim.x >> 6;
   const DecLayout L = make_dec_layout(unit, pairs, kLow);
@@ -571,6 +571,6 @@ __global__ void __launch_bounds__(kDecMaxPairs * 64)
       pair_sync(pair);
     }
     fresh = false;
-    decompress_pair_one<kLow>(t, slot, s, tab, L, init, role, pair, status);
+    decompress_pair_one<kLow>(t, slot, s, tab, L, init, role, pair, status, spin_limit);
   }
 }

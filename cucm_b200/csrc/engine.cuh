@@ -44,6 +44,7 @@ struct EngineConfig {
   int dec_pairs = 0;           // decoder chunks per CTA (0 = spread over all SMs first)
   int dec_tables = 0;          // decoder order 0/1 tables: 0 = shared memory where it fits, 1 = slot tables
   int cmp_ctas = 0;            // pipelined compressor CTAs per SM (0 = derived)
+  uint32_t spin_limit = 0;     // decoder: polls bounding the wait for a published round (0 = default)
 };
 
 cudaError_t upload_tables();  // once per device (current device)

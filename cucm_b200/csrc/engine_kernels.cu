@@ -624,12 +624,13 @@ cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t
     cudaError_t e = set_smem(kern, L.total);
     if (e != cudaSuccess) return e;
     const uint32_t grid = (nslots + (uint32_t)wpc - 1) / (uint32_t)wpc;
+    const uint32_t spin = cfg.spin_limit ? cfg.spin_limit : kDecSpinLimit;
     if (low)
       decompress_pair_kernel<true><<<grid, wpc * 64, L.total, stream>>>(d_tasks, ntasks, slots, nslots, init_tables,
-                                                                        d_init, d_queue, d_status, unit);
+                                                                        d_init, d_queue, d_status, unit, spin);
     else
       decompress_pair_kernel<false><<<grid, wpc * 64, L.total, stream>>>(d_tasks, ntasks, slots, nslots, init_tables,
-                                                                         d_init, d_queue, d_status, unit);
+                                                                         d_init, d_queue, d_status, unit, spin);
     return cudaGetLastError();
   }
   size_t smem = decompress_smem_bytes(unit, cfg.spec_bits);

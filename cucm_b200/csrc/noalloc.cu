@@ -1,9 +1,9 @@
 // noalloc.cu -- a compress entry point that allocates no memory.
 //
 // Some callers cannot allocate device memory at the moment they want to
-// compress: code running while a stream is being captured into a CUDA graph
-// (an allocation there fails or breaks the capture), plugins inside a host
-// application whose memory manager owns every device allocation, and
+// compress: plugins inside a host application whose memory manager owns
+// every device allocation (a cudaMalloc of their own would bypass its
+// accounting and can fail once the application has reserved the device), and
 // latency-critical paths that cannot afford cudaMalloc's implicit device
 // synchronisation.  cucm_compress_chunk_noalloc serves them: the caller
 // passes device input and output buffers, and the one piece of scratch the
@@ -13,17 +13,24 @@
 // Costs and rules of that array:
 //   * It is kSlotTableBytes (192.06 MiB: orders 0 and 1 by context, orders
 //     2..7 at 2^25 one-byte slots each) and belongs to this file's own
-//     module, so a process that never calls the entry point does not load it;
-//     once loaded, every GPU that ran the entry point holds it until exit.
+//     module.  Under lazy module loading (CUDA_MODULE_LOADING=LAZY, the CUDA
+//     12 default) the module, and with it the array, is loaded on a device
+//     only when this entry point first runs there; with
+//     CUDA_MODULE_LOADING=EAGER every context that loads libcucm.so reserves
+//     the 192.06 MiB at once.  Once loaded, a GPU holds it until the process
+//     exits.
 //   * One call codes one chunk: the array holds one chunk's tables, so input
 //     longer than the chunk size is rejected (CUCM_EINVAL).
 //   * Every call shares the array and it keeps the last call's contents; each
 //     call clears the tables on the caller's stream before its kernel runs.
 //     Calls that overlap on the GPU (different streams, no ordering between
 //     them) race on the array and produce garbage.  Serialise them.
+//   * The call is synchronous: it reads the payload length back and waits
+//     for the caller's stream before it returns.
 //   * The first call on a device does the set-up (symbol addresses, constant
 //     tables, kernel attributes) with that device current; make that first
-//     call before any stream capture begins.
+//     call before any stream capture begins.  A set-up that fails is tried
+//     again by the next call, except on a device that is not an sm_100 part.
 // The kernel is the pipelined compressor of engine_kernels.cu, instantiated
 // again in this module.
 #include <cuda_runtime.h>
@@ -57,8 +64,8 @@ static __device__ uint64_t g_noalloc_result;
 namespace {
 
 struct NoAllocDevice {
-  bool ready = false;
-  bool usable = false;
+  bool ready = false;     // set-up finished and succeeded
+  bool foreign = false;   // not an sm_100 device: never usable
   uint8_t *slot = nullptr;
   ModelInit *init = nullptr;
   uint32_t *status = nullptr;
@@ -72,14 +79,19 @@ std::mutex g_mu;
 // Once per device, with that device current: device addresses of the
 // file-scope scratch (the host-side names are stand-ins, not addresses),
 // the constant tables, the zero model and the kernel's shared-memory limit.
+// Only success is remembered, so a transient failure is retried next call.
 int noalloc_setup(int dev, NoAllocDevice *&out) {
   std::lock_guard<std::mutex> g(g_mu);
   NoAllocDevice &d = g_dev[dev];
   out = &d;
-  if (d.ready) return d.usable ? CUCM_OK : CUCM_ENODEV;
-  d.ready = true;
+  if (d.ready) return CUCM_OK;
+  if (d.foreign) return CUCM_ENODEV;
   cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major != 10) return CUCM_ENODEV;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return CUCM_ECUDA;
+  if (prop.major != 10) {
+    d.foreign = true;
+    return CUCM_ENODEV;
+  }
   if (cudaGetSymbolAddress((void **)&d.slot, g_noalloc_slot) != cudaSuccess) return CUCM_ECUDA;
   if (cudaGetSymbolAddress((void **)&d.init, g_noalloc_init) != cudaSuccess) return CUCM_ECUDA;
   if (cudaGetSymbolAddress((void **)&d.status, g_noalloc_status) != cudaSuccess) return CUCM_ECUDA;
@@ -96,7 +108,7 @@ int noalloc_setup(int dev, NoAllocDevice *&out) {
   if (cudaFuncSetAttribute((const void *)compress_fast_single_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return CUCM_ECUDA;
-  d.usable = true;
+  d.ready = true;
   return CUCM_OK;
 }
 
@@ -136,6 +148,7 @@ extern "C" int cucm_compress_chunk_noalloc(const uint8_t *d_in, uint64_t len, ui
   if (cudaStreamSynchronize(st) != cudaSuccess) return CUCM_ECUDA;
   *out_len = got;
   if (status & kDevBadTask) return CUCM_EINVAL;
+  if (status & ~(uint32_t)kDevOverflow) return CUCM_ECUDA;  // any other device status is an error
   if (got > cap) return CUCM_ENOSPC;
   return CUCM_OK;
 }

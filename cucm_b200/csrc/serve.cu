@@ -280,6 +280,7 @@ int run_tasks(cucm_server *s, Launch *l, const std::vector<ChunkTask> &tasks) {
   cfg.dec_pairs = s->tuning.dec_pairs;
   cfg.dec_tables = s->tuning.dec_tables;
   cfg.cmp_ctas = s->tuning.cmp_ctas;
+  cfg.spin_limit = s->tuning.dec_spin_limit;
   std::vector<ChunkTask> order = tasks;
   const bool dec = l->op == CUCM_OP_DECOMPRESS;
   std::stable_sort(order.begin(), order.end(), [&](const ChunkTask &a, const ChunkTask &b) {
@@ -571,6 +572,9 @@ void admit(cucm_server *s) {
     for (Req *r : cand) {
       if (r->prepared) continue;
       r->status = prepare(r);
+      // a request whose buffers alone exceed the buffer budget can never be
+      // admitted within it
+      if (!r->status && req_bytes(r) > s->buf_limit) r->status = CUCM_ENOMEM;
       if (r->status) bad.push_back(r);
     }
     if (!bad.empty()) {
@@ -744,6 +748,13 @@ int cucm_serve_poll(cucm_server *s, uint64_t id, int timeout_ms, int *status, ui
   if (out_n) *out_n = r->out_n;
   if (latency_ms) *latency_ms = r->t_done - r->t_submit;
   s->reqs.erase(it);
+  return CUCM_OK;
+}
+
+int cucm_server_set_queue_limit(cucm_server *s, uint32_t limit) {
+  if (!s) return CUCM_EINVAL;
+  std::lock_guard<std::mutex> g(s->mu);
+  s->max_queue = limit;
   return CUCM_OK;
 }
 

@@ -19,6 +19,7 @@ config0 (1 MiB text, 64 KiB chunks), config1 (256 MiB mixed, 1 MiB chunks,
 serving request stream: Poisson arrivals, sizes log-uniform in [1 KiB,
 16 MiB], 70% compress / 30% decompress, content drawn as in config2).
 """
+import concurrent.futures as _cf
 import ctypes
 import functools
 import os
@@ -105,6 +106,13 @@ def make(kind, n, seed):
     raise ValueError(kind)
 
 
+def _parallel(fn, items):
+    """fn over items on host threads (the generators release the GIL in C
+    and numpy); results in item order, identical to a serial run."""
+    with _cf.ThreadPoolExecutor(max(1, min(32, os.cpu_count() or 1))) as ex:
+        return list(ex.map(fn, items))
+
+
 def _derive(seed, i):
     return int(np.random.SeedSequence([seed, i]).generate_state(1, dtype=np.uint64)[0])
 
@@ -124,8 +132,11 @@ def config1(total=256 << 20, block=64 << 10):
     rng = np.random.default_rng(1)
     rng.shuffle(kinds)
     out = np.empty(nblocks * block, dtype=np.uint8)
-    for i, k in enumerate(kinds):
-        out[i * block:(i + 1) * block] = make(KINDS[k], block, _derive(1, i))
+
+    def fill(i):
+        out[i * block:(i + 1) * block] = make(KINDS[kinds[i]], block, _derive(1, i))
+
+    _parallel(fill, range(nblocks))
     return out, dict(chunksize=1 << 20, unit=128, prelearn=0, batch=100)
 
 
@@ -141,7 +152,7 @@ def config2(count=4096, lo=4096, hi=4 << 20, seed=2):
     content type each (0.5 text / 0.25 walk / 0.15 random / 0.1 runs);
     256 KiB chunks."""
     sizes, kinds = config2_sizes(count, lo, hi, seed)
-    bufs = [make(KINDS[k], int(s), _derive(seed, 1000 + i)) for i, (s, k) in enumerate(zip(sizes, kinds))]
+    bufs = _parallel(lambda i: make(KINDS[kinds[i]], int(sizes[i]), _derive(seed, 1000 + i)), range(count))
     return bufs, dict(chunksize=256 << 10, unit=128, prelearn=0, batch=100)
 
 

@@ -69,6 +69,9 @@ typedef struct cucm_tuning {
   int dec_pairs;       /* decoder chunks (warp pairs) per CTA, 0 = spread over all SMs first */
   int dec_tables;      /* decoder order 0/1 tables: 0 = shared memory where it fits, 1 = slot tables */
   int cmp_ctas;        /* pipelined compressor CTAs (chunks) per SM, 1 or 2; 0 = derived */
+  uint32_t dec_spin_limit; /* polls bounding the decoder's wait between its two warps; 0 = 2^27 (seconds).
+                            * When a wait runs out the call returns CUCM_ETIMEOUT and the context stays
+                            * usable; a small value makes that happen on purpose (tests). */
 } cucm_tuning;
 
 typedef struct cucm_ctx cucm_ctx;
@@ -177,6 +180,11 @@ int cucm_serve_submit(cucm_server *srv, int op, const uint8_t *in, uint64_t n, c
  * time from submit to completion; the id is then forgotten.  CUCM_PENDING
  * when it is still queued or running, CUCM_ENOTFOUND for an unknown id. */
 int cucm_serve_poll(cucm_server *srv, uint64_t id, int timeout_ms, int *status, uint64_t *out_n, double *latency_ms);
+/* Requests that may wait for admission at once (default 65536); submit
+ * returns CUCM_EBUSY beyond it.  A request whose own buffers exceed the
+ * server's buffer budget (a sixth of hbm_budget, at least 2 GiB) finishes
+ * with status CUCM_ENOMEM instead of being admitted over the budget. */
+int cucm_server_set_queue_limit(cucm_server *srv, uint32_t limit);
 int cucm_server_stats(cucm_server *srv, cucm_server_info *info);
 
 /* Device timing of the last call on this context, milliseconds (CUDA
@@ -218,22 +226,25 @@ int cucm_last_stats(cucm_ctx *ctx, cucm_stats *st);
 
 /* Compress one chunk without allocating any memory.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory when
- * they compress -- code running during a CUDA graph capture, plugins whose
- * host application owns every device allocation, and paths that cannot pay
- * for cudaMalloc's synchronisation.
+ * they compress -- plugins whose host application owns every device
+ * allocation through its own memory manager, and latency-critical paths that
+ * cannot pay for cudaMalloc's implicit device synchronisation.
  * d_in: `len` input bytes in device memory (1 <= len <= chunksize); the
  * result is that chunk's payload (coded bytes and flush byte) exactly as the
  * reference codes a chunk of that length in a stream of that chunk size and
  * unit, stale tail included when len < chunksize.  d_out: device buffer of
  * `cap` bytes; *out_len receives the payload size (CUCM_ENOSPC if it is
  * larger than cap).  unit: a multiple of 32 up to 256.  stream: a
- * cudaStream_t, or NULL for the legacy default stream; the call returns after
- * the stream has finished it.
+ * cudaStream_t, or NULL for the legacy default stream.  The call is
+ * synchronous: it returns after the stream has finished it.
  * The only scratch is a file-scope device array holding one chunk's tables
- * (192.06 MiB per GPU that calls this, kept until the process exits), so
- * input longer than one chunk is rejected with CUCM_EINVAL.  All calls share
- * that array; calls that overlap on the GPU race.  The first call on a device
- * does the set-up; make it before any stream capture begins. */
+ * (192.06 MiB per GPU, kept until the process exits), so input longer than
+ * one chunk is rejected with CUCM_EINVAL.  Under lazy module loading (the
+ * CUDA 12 default) a GPU reserves the array when this entry point first runs
+ * on it; with CUDA_MODULE_LOADING=EAGER every context that loads the library
+ * reserves it.  All calls share that array; calls that overlap on the GPU
+ * race.  The first call on a device does the set-up; make it before any
+ * stream capture begins. */
 int cucm_compress_chunk_noalloc(const uint8_t *d_in, uint64_t len, uint64_t chunksize, uint32_t unit,
                                 uint8_t *d_out, uint64_t cap, uint64_t *out_len, void *stream);
 

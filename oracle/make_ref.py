@@ -30,7 +30,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+# $CUCM_REFERENCE_DIR, else a sibling checkout named "reference" next to the repository.
+DEFAULT_REF = os.environ.get("CUCM_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 SOURCES = {
     "cucm_compress": "cucm_compress_v2.cu",
     "cucm_decompress": "cucm_decompress_v2.cu",
@@ -109,7 +110,7 @@ def build_gpu(ref_dir, force=False):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("CUCM_REFERENCE_DIR", DEFAULT_REF))
+    ap.add_argument("--reference", default=DEFAULT_REF)
     ap.add_argument("--gpu", action="store_true", help="also build the unmodified nvcc sm_100a binaries")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()

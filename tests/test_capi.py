@@ -53,6 +53,7 @@ def test_serve_calls_reject_bad_arguments(cucm_lib):
     assert cucm_lib.cucm_serve_submit(None, 0, None, 0, None, None, 0, ctypes.byref(rid)) == -1
     assert cucm_lib.cucm_serve_poll(None, 1, 0, None, None, None) == -1
     assert cucm_lib.cucm_server_destroy(None) == -1
+    assert cucm_lib.cucm_server_set_queue_limit(None, 4) == -1
 
 
 def test_default_params_match_reference_cli(cucm_lib):
@@ -78,9 +79,11 @@ def test_strerror(cucm_lib):
 
 
 def test_tuning_layout_and_autotune_arguments(cucm_lib):
-    # cucm_tuning: form, spec_bits, max_slots, (pad), hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas
-    assert ctypes.sizeof(cucm_b200.Tuning) == 40
+    # cucm_tuning: form, spec_bits, max_slots, (pad), hbm_budget, kernel, dec_pairs, dec_tables, cmp_ctas,
+    # dec_spin_limit, (pad)
+    assert ctypes.sizeof(cucm_b200.Tuning) == 48
     assert (cucm_b200.Tuning.dec_tables.offset, cucm_b200.Tuning.cmp_ctas.offset) == (32, 36)
+    assert cucm_b200.Tuning.dec_spin_limit.offset == 40
     assert cucm_lib.cucm_ctx_get_tuning(None, None) == -1
     t = cucm_b200.Tuning()
     p = cucm_b200.default_params()

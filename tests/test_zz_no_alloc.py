@@ -1,9 +1,9 @@
 """cucm_compress_chunk_noalloc: the compress entry point that allocates nothing.
 
-It serves callers that cannot allocate device memory while they compress
-(during a CUDA graph capture, inside a host application that owns every
-device allocation, on paths that cannot afford cudaMalloc's
-synchronisation).  Its only scratch is a file-scope device array holding one
+It serves callers that cannot allocate device memory while they compress:
+plugins inside a host application that owns every device allocation through
+its own memory manager, and paths that cannot afford cudaMalloc's implicit
+device synchronisation.  Its only scratch is a file-scope device array holding one
 chunk's tables, shared by every call.  This test calls it through the C ABI
 twice in a row on the same inputs -- the second call finds the first call's
 tables in that array and must start from clean ones -- and checks each
