@@ -124,6 +124,15 @@ __device__ inline DecSmem carve_dec(uint8_t *base, const DecLayout &L, int warp)
   return s;
 }
 
+// One slot state from the tables in HBM (L2-cached load).  The memory
+// clobber keeps the load where it is written: a round's gathers go out
+// before the previous round's record is stored to shared memory.
+__device__ __forceinline__ uint32_t ld_slot_state(const uint8_t *p) {
+  uint32_t v;
+  asm volatile("ld.global.cg.u8 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 // Warp-wide refill of the payload window so that it starts at or just below
 // payload byte `at`, on a 16-byte boundary of the payload's address (so the
 // window base may lie up to 15 bytes before the payload).  Only 16-byte
@@ -432,23 +441,30 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
   int r = 0;          // 0 or 4
   uint32_t published = 0;
 
+  // A round's keys and frozen slot states.  After a round is decoded the
+  // next round's gathers go out at once (within a unit: the unit end writes
+  // the slot tables), and the decoded round is recorded and published while
+  // they are in flight.
+  BitKeys kk;
+  uint32_t st[kOrders];
+  auto gather = [&](BitKeys &k, uint32_t *sv, uint32_t cur_, int r_, uint64_t hist_) {
+    const uint32_t h0 = (1u << (r_ + depth)) | (cur_ << depth) | pbits;
+    bit_keys64(h0, hist_, k);
+    if (kLow) {
+      sv[0] = s.t01[k.k[0]];
+      sv[1] = s.t01[kOrder1Off + k.k[1]];
+    }
+CUCM_UNROLL
+    for (int o = kLow ? 2 : 0; o < kOrders; o++) sv[o] = ld_slot_state(slot + table_offset(o) + k.k[o]);
+  };
+
   for (uint64_t base = 0; base < nbits; base += (uint64_t)U) {
     const int nunit = (int)(nbits - base < (uint64_t)U ? nbits - base : (uint64_t)U);
     const int nr = nunit >> 2;
     int obyte = 0;
+    gather(kk, st, cur, r, hist);
     for (int rd = 0; rd < nr; rd++) {
       if ((long long)ioff + 16 > wbase + kDecWin) wbase = dec_refill(s.win, pay, plen, ioff, lane);
-      // keys and gathers of this lane's node
-      const uint32_t h0 = (1u << (r + depth)) | (cur << depth) | pbits;
-      BitKeys kk;
-      bit_keys64(h0, hist, kk);
-      uint32_t st[kOrders];
-      if (kLow) {
-        st[0] = s.t01[kk.k[0]];
-        st[1] = s.t01[kOrder1Off + kk.k[1]];
-      }
-CUCM_UNROLL
-      for (int o = kLow ? 2 : 0; o < kOrders; o++) st[o] = __ldcg(slot + table_offset(o) + kk.k[o]);
       // stretch, mixer context, mixer output (cucm_decompress_v2.cu:774-809)
       const int c1 = (int)(hist & 0xffu);
       int smp[kOrders];
@@ -487,32 +503,41 @@ CUCM_UNROLL
         n = 2 * n + 1 + y;
         f = y ? fb : fa;
       }
-      // the path's lanes record their bit for the updating warp
-      if (recorder && pbits == (nib >> (4 - depth))) {
-        const int i = depth;
-        uint4 *k4 = reinterpret_cast<uint4 *>(s.rk + (rd * 4 + i) * kOrders);
-        k4[0] = make_uint4(kk.k[0], kk.k[1], kk.k[2], kk.k[3]);
-        k4[1] = make_uint4(kk.k[4], kk.k[5], kk.k[6], kk.k[7]);
-        uint2 sv;
-        sv.x = st[0] | (st[1] << 8) | (st[2] << 16) | (st[3] << 24);
-        sv.y = st[4] | (st[5] << 8) | (st[6] << 16) | (st[7] << 24);
-        *reinterpret_cast<uint2 *>(s.rs + (rd * 4 + i) * kOrders) = sv;
-        uint4 m;
-        m.x = (uint32_t)(smp[0] & 0xffff) | ((uint32_t)smp[1] << 16);
-        m.y = (uint32_t)(smp[2] & 0xffff) | ((uint32_t)smp[3] << 16);
-        m.z = (uint32_t)(smp[4] & 0xffff) | ((uint32_t)smp[5] << 16);
-        m.w = (uint32_t)(smp[6] & 0xffff) | ((uint32_t)smp[7] << 16);
-        *reinterpret_cast<uint4 *>(s.rsmp + (rd * 4 + i) * kOrders) = m;
-        s.rpc[rd * 4 + i] = (uint32_t)pr_node | ((uint32_t)cxt << 16) | (((nib >> (3 - i)) & 1u) << 24);
-      }
+      // the round's record, kept in registers while the next round's
+      // gathers go out
+      const bool on_path = recorder && pbits == (nib >> (4 - depth));
+      const uint4 rk0 = make_uint4(kk.k[0], kk.k[1], kk.k[2], kk.k[3]);
+      const uint4 rk1 = make_uint4(kk.k[4], kk.k[5], kk.k[6], kk.k[7]);
+      const uint2 rsv = make_uint2(st[0] | (st[1] << 8) | (st[2] << 16) | (st[3] << 24),
+                                   st[4] | (st[5] << 8) | (st[6] << 16) | (st[7] << 24));
+      const uint4 rm = make_uint4((uint32_t)(smp[0] & 0xffff) | ((uint32_t)smp[1] << 16),
+                                  (uint32_t)(smp[2] & 0xffff) | ((uint32_t)smp[3] << 16),
+                                  (uint32_t)(smp[4] & 0xffff) | ((uint32_t)smp[5] << 16),
+                                  (uint32_t)(smp[6] & 0xffff) | ((uint32_t)smp[7] << 16));
+      const uint32_t rpc = (uint32_t)pr_node | ((uint32_t)cxt << 16) | (((nib >> (3 - depth)) & 1u) << 24);
       cur = (cur << 4) | nib;
       r += 4;
+      bool byte_done = false;
       if (r == 8) {
-        if (lane == 0) s.outb[obyte] = (uint8_t)cur;
-        obyte++;
+        byte_done = true;
         hist = (hist << 8) | cur;
         cur = 0;
         r = 0;
+      }
+      if (rd + 1 < nr) gather(kk, st, cur, r, hist);
+      // the path's lanes record their bit for the updating warp
+      if (on_path) {
+        const int i = depth;
+        uint4 *k4 = reinterpret_cast<uint4 *>(s.rk + (rd * 4 + i) * kOrders);
+        k4[0] = rk0;
+        k4[1] = rk1;
+        *reinterpret_cast<uint2 *>(s.rs + (rd * 4 + i) * kOrders) = rsv;
+        *reinterpret_cast<uint4 *>(s.rsmp + (rd * 4 + i) * kOrders) = rm;
+        s.rpc[rd * 4 + i] = rpc;
+      }
+      if (byte_done) {
+        if (lane == 0) s.outb[obyte] = (uint8_t)hist;
+        obyte++;
       }
       __syncwarp();
       published++;

@@ -156,6 +156,18 @@ def config2(count=4096, lo=4096, hi=4 << 20, seed=2):
     return bufs, dict(chunksize=256 << 10, unit=128, prelearn=0, batch=100)
 
 
+def config2_sample(k=512, count=4096):
+    """A stratified sample of config2's buffers: every (count / k)-th buffer
+    in size order, the largest included.  Sorted buffer indices."""
+    sizes, _ = config2_sizes(count)
+    order = sorted(range(count), key=lambda i: (int(sizes[i]), i))
+    step = max(1, count // k)
+    pick = order[::step][:k]
+    if order[-1] not in pick:
+        pick[-1] = order[-1]
+    return sorted(pick)
+
+
 def config4(count, offered_gbps, lo=1024, hi=16 << 20, seed=4):
     """A serving request stream of `count` requests at an offered load of
     `offered_gbps` GB/s: Poisson arrivals (exponential gaps whose mean is the

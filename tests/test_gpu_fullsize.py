@@ -54,16 +54,6 @@ def many4096():
     return bufs, p, m
 
 
-def stratified_sample(lens, k=512):
-    """Every (n / k)-th buffer in size order, the largest included."""
-    order = sorted(range(len(lens)), key=lambda i: (lens[i], i))
-    step = max(1, len(order) // k)
-    pick = order[::step][:k]
-    if order[-1] not in pick:
-        pick[-1] = order[-1]
-    return sorted(pick)
-
-
 def test_many4096_batched_matches_reference(gpu_ctx, many4096):
     bufs, p, m = many4096
     gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT)
@@ -76,7 +66,7 @@ def test_many4096_batched_matches_reference(gpu_ctx, many4096):
 
 def test_many4096_plain_sample_matches_reference(gpu_ctx, many4096):
     bufs, p, m = many4096
-    pick = stratified_sample(m["input_lens"])
+    pick = W.config2_sample(512)
     lens = m["input_lens"]
     assert len(pick) == 512
     assert min(lens[i] for i in pick) == min(lens) and max(lens[i] for i in pick) == max(lens)
