@@ -105,6 +105,28 @@ SIGNATURES = [
                                            ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, _u64p]),
     ("cucm_decompress_batch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                              ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64]),
+    ("cucm_model_prelearn", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("cucm_model_from_container", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("cucm_model_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("cucm_compress_batch_model", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                                 _u64p]),
+    ("cucm_decompress_batch_model", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                                   ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_uint64]),
+    ("cucm_compress_batch_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                               ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                               _u64p]),
+    ("cucm_frame_bodies", ctypes.c_int, [ctypes.POINTER(Params), ctypes.c_uint64, ctypes.c_uint32,
+                                         ctypes.POINTER(ctypes.c_void_p), _u64p, ctypes.POINTER(ctypes.c_uint32),
+                                         ctypes.c_void_p, ctypes.c_uint64, _u64p]),
+    ("cucm_frame_bodies_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_uint64,
+                                             ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), _u64p,
+                                             ctypes.POINTER(ctypes.c_uint32), ctypes.c_void_p, ctypes.c_uint64,
+                                             _u64p]),
+    ("cucm_decompress_range_dev", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                                 ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
+                                                 ctypes.c_uint64, _u64p]),
     ("cucm_compress_many", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), _u64p,
                                           ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p), _u64p, _u64p,
                                           ctypes.POINTER(ctypes.c_int)]),
@@ -191,6 +213,45 @@ def _buf(data):
     b = bytes(data)
     cb = ctypes.create_string_buffer(b, len(b)) if b else ctypes.create_string_buffer(1)
     return ctypes.addressof(cb), len(b), cb
+
+
+class Model:
+    """An initial model (the reference's sm_init / mixer_init): trained by
+    the prelearn pass over a prefix, or read from a container's prelearn
+    block.  Host memory only; pass it to compress_batch / decompressbatch."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def prelearn(cls, prefix):
+        ptr, n, keep = _buf(prefix)
+        h = ctypes.c_void_p()
+        rc = lib().cucm_model_prelearn(ptr, n, ctypes.byref(h))
+        if rc:
+            raise CucmError(rc, "cucm_model_prelearn")
+        return cls(h)
+
+    @classmethod
+    def from_container(cls, blob):
+        """The container's model, or None when it has no prelearn block."""
+        ptr, n, keep = _buf(blob)
+        h = ctypes.c_void_p()
+        rc = lib().cucm_model_from_container(ptr, n, ctypes.byref(h))
+        if rc:
+            raise CucmError(rc, "cucm_model_from_container")
+        return cls(h) if h.value else None
+
+    def close(self):
+        if self._h:
+            lib().cucm_model_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:
@@ -290,23 +351,27 @@ class Context:
             raise CucmError(rc, "cucm_decompress_dev")
         return got.value
 
-    def compress_batch(self, data, chunksize, unitlength=128):
+    def compress_batch(self, data, chunksize, unitlength=128, model=None):
+        """Batch body of `data` (compress_batch); `model` is sm_init/mixer_init
+        (a Model, or None for the zero model)."""
         ptr, n, keep = _buf(data)
         nchunks = (n + chunksize - 1) // chunksize
         cap = nchunks * (4 + 32 * chunksize + 1) + 16
         out = ctypes.create_string_buffer(max(cap, 1))
         got = ctypes.c_uint64()
-        rc = lib().cucm_compress_batch(self._h, ptr, n, chunksize, unitlength, out, cap, ctypes.byref(got))
+        rc = lib().cucm_compress_batch_model(self._h, ptr, n, chunksize, unitlength, model._h if model else None,
+                                             out, cap, ctypes.byref(got))
         if rc:
-            raise CucmError(rc, "cucm_compress_batch")
+            raise CucmError(rc, "cucm_compress_batch_model")
         return out.raw[:got.value]
 
-    def decompressbatch(self, body, out_size, chunksize, unitlength=128):
+    def decompressbatch(self, body, out_size, chunksize, unitlength=128, model=None):
         ptr, n, keep = _buf(body)
         out = ctypes.create_string_buffer(max(out_size, 1))
-        rc = lib().cucm_decompress_batch(self._h, ptr, n, chunksize, unitlength, out, out_size)
+        rc = lib().cucm_decompress_batch_model(self._h, ptr, n, chunksize, unitlength, model._h if model else None,
+                                               out, out_size)
         if rc:
-            raise CucmError(rc, "cucm_decompress_batch")
+            raise CucmError(rc, "cucm_decompress_batch_model")
         return out.raw[:out_size]
 
     def compress_many(self, buffers, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
@@ -399,6 +464,25 @@ class Context:
         st = Stats()
         lib().cucm_last_stats(self._h, ctypes.byref(st))
         return dict(device_ms=st.device_ms, kernel_ms=st.kernel_ms, launches=st.launches, chunks=st.chunks)
+
+
+def frame_bodies(bodies, counts, orig_size, chunksize=1 << 20, unit=128, batch=100):
+    """The container of a stream whose chunks were coded in consecutive
+    pieces (cucm_frame_bodies; host buffers, no device work): bodies[i] is the
+    batch body of counts[i] consecutive chunks."""
+    p = default_params(chunksize, unit, 0, batch)
+    k = len(bodies)
+    bufs = [_buf(b) for b in bodies]
+    ptrs = (ctypes.c_void_p * k)(*[b[0] for b in bufs])
+    ns = (ctypes.c_uint64 * k)(*[b[1] for b in bufs])
+    cs = (ctypes.c_uint32 * k)(*counts)
+    cap = 64 + 4 * ((sum(counts) + batch - 1) // batch) + sum(b[1] for b in bufs)
+    out = ctypes.create_string_buffer(cap)
+    got = ctypes.c_uint64()
+    rc = lib().cucm_frame_bodies(ctypes.byref(p), orig_size, k, ptrs, ns, cs, out, cap, ctypes.byref(got))
+    if rc:
+        raise CucmError(rc, "cucm_frame_bodies")
+    return out.raw[:got.value]
 
 
 _default_ctx = None

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -33,6 +34,11 @@ namespace {
 #include "container.cuh"
 
 }  // namespace
+
+struct cucm_model {
+  cucm::ModelInit init;
+  std::vector<uint8_t> image;  // slot tables in the device layout
+};
 
 struct cucm_ctx {
   int device = 0;
@@ -82,6 +88,16 @@ void zero_model(ModelInit &mi) {
   for (int o = 0; o < kOrders; o++)
     for (int s = 0; s < 256; s++) mi.statep[o][s] = 1u << 31;
   std::memset(mi.w, 0, sizeof mi.w);
+}
+
+// A caller's model (sm_init / mixer_init), or the zero model for null.
+void model_source(const cucm_model *m, ModelSource &ms) {
+  if (m) {
+    ms.init = m->init;
+    ms.image = &m->image;
+  } else {
+    zero_model(ms.init);
+  }
 }
 
 uint64_t budget_bytes(cucm_ctx *c) {
@@ -789,9 +805,78 @@ int cucm_decompress_dev(cucm_ctx *c, const uint8_t *in, uint64_t n, uint8_t *out
   return decompress_containers(c, 1, &in, &n, &out, &cap, out_n, &st, true);
 }
 
-int cucm_compress_batch(cucm_ctx *c, const uint8_t *in, uint64_t n, uint64_t chunksize, uint32_t unit, uint8_t *out,
-                        uint64_t cap, uint64_t *out_n) {
-  if (!c || !out_n || (!in && n)) return CUCM_EINVAL;
+int cucm_model_prelearn(const uint8_t *prefix, uint64_t n, cucm_model **out) {
+  if (!out || (!prefix && n)) return CUCM_EINVAL;
+  *out = nullptr;
+  std::unique_ptr<cucm_model> m(new (std::nothrow) cucm_model());
+  if (!m) return CUCM_ENOMEM;
+  try {
+    HostModel hm;
+    hm.prelearn_train(prefix, n);
+    hm.to_device(m->image, m->init);
+  } catch (const std::bad_alloc &) {
+    return CUCM_ENOMEM;
+  }
+  *out = m.release();
+  return CUCM_OK;
+}
+
+int cucm_model_from_container(const uint8_t *in, uint64_t n, cucm_model **out) {
+  if (!out) return CUCM_EINVAL;
+  *out = nullptr;
+  Parsed ph;
+  int rc = parse_header(in, n, ph);
+  if (rc) return rc;
+  if (!ph.prelearn) return CUCM_OK;
+  std::unique_ptr<cucm_model> m(new (std::nothrow) cucm_model());
+  if (!m) return CUCM_ENOMEM;
+  try {
+    HostModel hm;
+    std::vector<uint8_t> pre(ph.prelearn);
+    if (ph.coded)
+      hm.prelearn_decode(in + kHeaderBytes, ph.pl_len, pre.data(), ph.prelearn);
+    else
+      hm.prelearn_train(in + kHeaderBytes, ph.prelearn);
+    hm.to_device(m->image, m->init);
+  } catch (const std::bad_alloc &) {
+    return CUCM_ENOMEM;
+  }
+  *out = m.release();
+  return CUCM_OK;
+}
+
+int cucm_model_destroy(cucm_model *m) {
+  if (!m) return CUCM_EINVAL;
+  delete m;
+  return CUCM_OK;
+}
+
+// compress_batch of n bytes in device memory into a device body (C big-endian
+// end offsets + payloads); `staged`: d_in is the context's own staging copy.
+static int compress_body(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint64_t chunksize, uint32_t unit,
+                         const cucm_model *m, uint8_t *d_out, uint64_t cap, uint64_t *out_n, uint8_t *h_out) {
+  ModelSource ms;
+  model_source(m, ms);
+  Encoded e;
+  int rc = encode_chunks(c, {Seg{d_in, n}}, chunksize, unit, ms, c->d_body.cap + c->d_out.cap, e);
+  const uint64_t body_n = rc ? 0 : layout_body(e, 0, 0xffff, false, nullptr, nullptr);
+  *out_n = body_n;
+  if (!rc && body_n > cap) rc = CUCM_ENOSPC;
+  if (!rc && body_n) {
+    uint8_t *dst = d_out;
+    if (h_out) {
+      CK(c->d_out.ensure(body_n));
+      dst = c->d_out.as<uint8_t>();
+    }
+    std::vector<PackEntry> pe;
+    layout_body(e, 0, 0xffff, false, dst, &pe);
+    rc = pack_bodies(c, pe);
+    if (!rc && h_out) CK(cudaMemcpyAsync(h_out, dst, body_n, cudaMemcpyDeviceToHost, c->stream));
+  }
+  return rc;
+}
+
+static int batch_args(uint64_t n, uint64_t chunksize, uint32_t unit) {
   cucm_params p;
   cucm_default_params(&p);
   p.chunksize = chunksize;
@@ -799,34 +884,41 @@ int cucm_compress_batch(cucm_ctx *c, const uint8_t *in, uint64_t n, uint64_t chu
   p.batch = 0xffff;
   int rc = check_params(&p, n);
   if (rc) return rc;
-  uint64_t nchunks = (n + chunksize - 1) / chunksize;
-  if (nchunks > 0xffff) return CUCM_EINVAL;
+  return (n + chunksize - 1) / chunksize > 0xffff ? CUCM_EINVAL : CUCM_OK;
+}
+
+int cucm_compress_batch_model(cucm_ctx *c, const uint8_t *in, uint64_t n, uint64_t chunksize, uint32_t unit,
+                              const cucm_model *m, uint8_t *out, uint64_t cap, uint64_t *out_n) {
+  if (!c || !out_n || (!in && n)) return CUCM_EINVAL;
+  int rc = batch_args(n, chunksize, unit);
+  if (rc) return rc;
   std::lock_guard<std::mutex> g(c->mu);
   CK(cudaSetDevice(c->device));
-  ModelSource ms;
-  zero_model(ms.init);
   timing_begin(c);
   CK(c->d_body.ensure(n ? n : 1));
   if (n) CK(cudaMemcpyAsync(c->d_body.p, in, n, cudaMemcpyHostToDevice, c->stream));
-  Encoded e;
-  rc = encode_chunks(c, {Seg{c->d_body.as<uint8_t>(), n}}, chunksize, unit, ms, c->d_body.cap + c->d_out.cap, e);
-  const uint64_t body_n = rc ? 0 : layout_body(e, 0, 0xffff, false, nullptr, nullptr);
-  *out_n = body_n;
-  if (!rc && body_n > cap) rc = CUCM_ENOSPC;
-  if (!rc && body_n) {
-    CK(c->d_out.ensure(body_n));
-    std::vector<PackEntry> pe;
-    layout_body(e, 0, 0xffff, false, c->d_out.as<uint8_t>(), &pe);
-    rc = pack_bodies(c, pe);
-    if (!rc) CK(cudaMemcpyAsync(out, c->d_out.p, body_n, cudaMemcpyDeviceToHost, c->stream));
-  }
+  rc = compress_body(c, c->d_body.as<uint8_t>(), n, chunksize, unit, m, nullptr, cap, out_n, out);
   timing_end(c);
   CK(cudaStreamSynchronize(c->stream));
   return rc;
 }
 
-int cucm_decompress_batch(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uint64_t chunksize, uint32_t unit,
-                          uint8_t *out, uint64_t out_n) {
+int cucm_compress_batch_dev(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint64_t chunksize, uint32_t unit,
+                            const cucm_model *m, uint8_t *d_out, uint64_t cap, uint64_t *out_n) {
+  if (!c || !out_n || (!d_in && n) || !d_out) return CUCM_EINVAL;
+  int rc = batch_args(n, chunksize, unit);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(c->mu);
+  CK(cudaSetDevice(c->device));
+  timing_begin(c);
+  rc = compress_body(c, d_in, n, chunksize, unit, m, d_out, cap, out_n, nullptr);
+  timing_end(c);
+  CK(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+int cucm_decompress_batch_model(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uint64_t chunksize,
+                                uint32_t unit, const cucm_model *m, uint8_t *out, uint64_t out_n) {
   if (!c || !body || (!out && out_n)) return CUCM_EINVAL;
   if (chunksize == 0 || unit < 32 || unit > (uint32_t)kMaxUnit || unit % 32) return CUCM_EINVAL;
   uint64_t nchunks = (out_n + chunksize - 1) / chunksize;
@@ -836,7 +928,7 @@ int cucm_decompress_batch(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uin
   std::lock_guard<std::mutex> g(c->mu);
   CK(cudaSetDevice(c->device));
   ModelSource ms;
-  zero_model(ms.init);
+  model_source(m, ms);
   timing_begin(c);
   CK(c->d_body.ensure(body_n ? body_n : 1));
   CK(cudaMemcpyAsync(c->d_body.p, body, body_n, cudaMemcpyHostToDevice, c->stream));
@@ -847,6 +939,209 @@ int cucm_decompress_batch(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uin
   jb.cs = chunksize;
   rc = decode_jobs(c, {jb}, unit, ms, c->d_body.cap + c->d_out.cap);
   if (!rc && out_n) CK(cudaMemcpyAsync(out, c->d_out.p, out_n, cudaMemcpyDeviceToHost, c->stream));
+  timing_end(c);
+  CK(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+int cucm_compress_batch(cucm_ctx *c, const uint8_t *in, uint64_t n, uint64_t chunksize, uint32_t unit, uint8_t *out,
+                        uint64_t cap, uint64_t *out_n) {
+  return cucm_compress_batch_model(c, in, n, chunksize, unit, nullptr, out, cap, out_n);
+}
+
+int cucm_decompress_batch(cucm_ctx *c, const uint8_t *body, uint64_t body_n, uint64_t chunksize, uint32_t unit,
+                          uint8_t *out, uint64_t out_n) {
+  return cucm_decompress_batch_model(c, body, body_n, chunksize, unit, nullptr, out, out_n);
+}
+
+namespace {
+
+// Payload extents of every chunk of `nbodies` batch bodies (C_i end offsets +
+// payloads each), in stream order, from the bodies' offset tables (`tables`,
+// host copies); src[k] points into the body, host or device memory alike.
+int bodies_extents(uint32_t nbodies, const uint8_t *const *bodies, const uint64_t *body_ns,
+                   const uint32_t *counts, const std::vector<std::vector<uint8_t>> &tables,
+                   std::vector<uint64_t> &lens, std::vector<const uint8_t *> &src) {
+  for (uint32_t i = 0; i < nbodies; i++) {
+    const uint64_t C = counts[i];
+    if (C == 0) continue;
+    if (body_ns[i] < 4 * C || tables[i].size() < 4 * C) return CUCM_EFORMAT;
+    uint64_t prev = 0;
+    for (uint64_t k = 0; k < C; k++) {
+      const uint64_t endv = get_be32(&tables[i][4 * k]);
+      if (endv + 1 < 4 * C) return CUCM_EFORMAT;
+      const uint64_t end = endv + 1 - 4 * C;
+      if (end < prev || 4 * C + end > body_ns[i]) return CUCM_EFORMAT;
+      lens.push_back(end - prev);
+      src.push_back(bodies[i] + 4 * C + prev);
+      prev = end;
+    }
+  }
+  return CUCM_OK;
+}
+
+int frame_check(const cucm_params *p, uint64_t orig_size, uint32_t nbodies, const uint8_t *const *bodies,
+                const uint64_t *body_ns, const uint32_t *counts, uint64_t *out_n) {
+  if (!p || !out_n || (nbodies && (!bodies || !body_ns || !counts))) return CUCM_EINVAL;
+  if (p->prelearn) return CUCM_EINVAL;  // a prelearn block belongs to the stream's writer
+  int rc = check_params(p, orig_size);
+  if (rc) return rc;
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < nbodies; i++) {
+    if (!bodies[i] && counts[i]) return CUCM_EINVAL;
+    total += counts[i];
+  }
+  return total == (orig_size + p->chunksize - 1) / p->chunksize ? CUCM_OK : CUCM_EINVAL;
+}
+
+}  // namespace
+
+int cucm_frame_bodies(const cucm_params *p, uint64_t orig_size, uint32_t nbodies, const uint8_t *const *bodies,
+                      const uint64_t *body_ns, const uint32_t *counts, uint8_t *out, uint64_t cap,
+                      uint64_t *out_n) {
+  int rc = frame_check(p, orig_size, nbodies, bodies, body_ns, counts, out_n);
+  if (rc) return rc;
+  std::vector<std::vector<uint8_t>> tables(nbodies);
+  for (uint32_t i = 0; i < nbodies; i++)
+    if (counts[i]) tables[i].assign(bodies[i], bodies[i] + std::min<uint64_t>(4ull * counts[i], body_ns[i]));
+  std::vector<uint64_t> lens;
+  std::vector<const uint8_t *> src;
+  rc = bodies_extents(nbodies, bodies, body_ns, counts, tables, lens, src);
+  if (rc) return rc;
+  std::vector<uint8_t> hdr;
+  std::unique_ptr<HostModel> hm;
+  rc = make_header(nullptr, orig_size, p, hdr, hm);
+  if (rc) return rc;
+  const uint64_t body = layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, nullptr, nullptr);
+  *out_n = hdr.size() + body;
+  if (*out_n > cap) return CUCM_ENOSPC;
+  if (!out) return CUCM_EINVAL;
+  std::memcpy(out, hdr.data(), hdr.size());
+  std::vector<PackEntry> pe;
+  layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, out + hdr.size(), &pe);
+  for (const PackEntry &e : pe) {
+    if (e.len) std::memcpy(e.base + e.dst, e.src, e.len);
+    put_be32(e.base + e.table_at, e.end_value);
+    if (e.size_at != ~0ull) {
+      uint8_t *z = e.base + e.size_at;
+      z[0] = (uint8_t)e.batch_size;
+      z[1] = (uint8_t)(e.batch_size >> 8);
+      z[2] = (uint8_t)(e.batch_size >> 16);
+      z[3] = (uint8_t)(e.batch_size >> 24);
+    }
+  }
+  return CUCM_OK;
+}
+
+int cucm_frame_bodies_dev(cucm_ctx *c, const cucm_params *p, uint64_t orig_size, uint32_t nbodies,
+                          const uint8_t *const *bodies, const uint64_t *body_ns, const uint32_t *counts,
+                          uint8_t *d_out, uint64_t cap, uint64_t *out_n) {
+  if (!c) return CUCM_EINVAL;
+  int rc = frame_check(p, orig_size, nbodies, bodies, body_ns, counts, out_n);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(c->mu);
+  CK(cudaSetDevice(c->device));
+  timing_begin(c);
+  std::vector<std::vector<uint8_t>> tables(nbodies);
+  for (uint32_t i = 0; i < nbodies; i++) {
+    tables[i].resize(counts[i] ? std::min<uint64_t>(4ull * counts[i], body_ns[i]) : 0);
+    if (!tables[i].empty())
+      CK(cudaMemcpyAsync(tables[i].data(), bodies[i], tables[i].size(), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<uint64_t> lens;
+  std::vector<const uint8_t *> src;
+  rc = bodies_extents(nbodies, bodies, body_ns, counts, tables, lens, src);
+  if (rc) return rc;
+  std::vector<uint8_t> hdr;
+  std::unique_ptr<HostModel> hm;
+  rc = make_header(nullptr, orig_size, p, hdr, hm);
+  if (rc) return rc;
+  const uint64_t body = layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, nullptr, nullptr);
+  *out_n = hdr.size() + body;
+  if (*out_n > cap) return CUCM_ENOSPC;
+  if (!d_out) return CUCM_EINVAL;
+  CK(cudaMemcpyAsync(d_out, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, c->stream));
+  std::vector<PackEntry> pe;
+  layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, d_out + hdr.size(), &pe);
+  rc = pack_bodies(c, pe);
+  timing_end(c);
+  CK(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+int cucm_decompress_range_dev(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint64_t first, uint64_t count,
+                              uint8_t *d_out, uint64_t cap, uint64_t *out_n) {
+  if (!c || !d_in || !out_n) return CUCM_EINVAL;
+  std::lock_guard<std::mutex> g(c->mu);
+  CK(cudaSetDevice(c->device));
+  *out_n = 0;
+  if (n < kHeaderBytes) return CUCM_EFORMAT;
+  uint8_t hb[kHeaderBytes];
+  CK(cudaMemcpy(hb, d_in, kHeaderBytes, cudaMemcpyDeviceToHost));
+  Parsed ph;
+  int rc = parse_header(hb, n, ph);  // also checks that the prelearn block lies inside the n bytes
+  if (rc) return rc;
+  const uint64_t body_off = kHeaderBytes + ph.pl_len;
+  const uint64_t out_body = ph.total - ph.prelearn;
+  const uint64_t nchunks = (out_body + ph.cs - 1) / ph.cs;
+  if (first > nchunks || count > nchunks - first) return CUCM_EINVAL;
+  const uint64_t want = count ? std::min<uint64_t>(ph.cs * count, out_body - first * ph.cs) : 0;
+  *out_n = want;
+  if (want > cap) return CUCM_ENOSPC;
+  if (!count) return CUCM_OK;
+  if (!d_out) return CUCM_EINVAL;
+  ModelSource ms;
+  std::vector<uint8_t> image;
+  if (ph.prelearn) {
+    std::vector<uint8_t> blk(ph.pl_len), pre(ph.prelearn);
+    CK(cudaMemcpy(blk.data(), d_in + kHeaderBytes, ph.pl_len, cudaMemcpyDeviceToHost));
+    HostModel hm;
+    if (ph.coded)
+      hm.prelearn_decode(blk.data(), ph.pl_len, pre.data(), ph.prelearn);
+    else
+      hm.prelearn_train(blk.data(), ph.prelearn);
+    hm.to_device(image, ms.init);
+    ms.image = &image;
+  } else {
+    zero_model(ms.init);
+  }
+  // walk the batches: their size fields, and the tables of those in range
+  DecJob jb;
+  jb.d_body = d_in + body_off;
+  jb.total = out_body - first * ph.cs;
+  jb.cs = ph.cs;
+  jb.d_out = d_out;
+  uint64_t r = 0;
+  const uint64_t body_n = n - body_off;
+  for (uint64_t k0 = 0; k0 < first + count; k0 += ph.batch) {
+    const uint64_t k1 = std::min<uint64_t>(k0 + ph.batch, nchunks), C = k1 - k0;
+    uint8_t sz[4];
+    if (r + 4 > body_n) return CUCM_EFORMAT;
+    CK(cudaMemcpy(sz, d_in + body_off + r, 4, cudaMemcpyDeviceToHost));
+    const uint64_t bsz = get_le32(sz);
+    r += 4;
+    if (bsz < 4 * C || r + bsz > body_n) return CUCM_EFORMAT;
+    if (k1 > first) {
+      std::vector<uint8_t> tab(4 * C);
+      CK(cudaMemcpy(tab.data(), d_in + body_off + r, 4 * C, cudaMemcpyDeviceToHost));
+      uint64_t start = 0;
+      for (uint64_t k = k0; k < k1; k++) {
+        const uint64_t endv = get_be32(&tab[4 * (k - k0)]);
+        if (endv + 1 < 4 * C) return CUCM_EFORMAT;
+        const uint64_t end = endv + 1 - 4 * C;
+        if (end < start || end > bsz - 4 * C) return CUCM_EFORMAT;
+        if (k >= first && k < first + count) {
+          jb.off.push_back(r + 4 * C + start);
+          jb.len.push_back(end - start);
+        }
+        start = end;
+      }
+    }
+    r += bsz;
+  }
+  timing_begin(c);
+  rc = decode_jobs(c, {jb}, ph.unit, ms, c->d_body.cap + c->d_out.cap);
   timing_end(c);
   CK(cudaStreamSynchronize(c->stream));
   return rc;

@@ -108,7 +108,8 @@ int cucm_decompress_dev(cucm_ctx *ctx, const uint8_t *d_in, uint64_t n, uint8_t 
 
 /* One batch body, no container header: `n` bytes of input split into
  * chunks of `chunksize`, coded from the zero model (compress_batch,
- * cucm_compress_v2.cu:990-1149 with sm_init = mixer_init = NULL).  Output is
+ * cucm_compress_v2.cu:990-1149 with sm_init = mixer_init = NULL; see
+ * cucm_compress_batch_model for a prelearned model).  Output is
  * the batch body the reference writes after its u32 size field: C big-endian
  * u32 chunk end offsets followed by the chunk payloads. */
 int cucm_compress_batch(cucm_ctx *ctx, const uint8_t *in, uint64_t n, uint64_t chunksize, uint32_t unit,
@@ -118,6 +119,54 @@ int cucm_compress_batch(cucm_ctx *ctx, const uint8_t *in, uint64_t n, uint64_t c
  * number of original bytes. */
 int cucm_decompress_batch(cucm_ctx *ctx, const uint8_t *body, uint64_t body_n, uint64_t chunksize, uint32_t unit,
                           uint8_t *out, uint64_t out_n);
+
+/* An initial model: what every chunk of a stream starts from.  The
+ * reference's compress_batch / decompressbatch take it as sm_init and
+ * mixer_init (cucm_compress_v2.cu:990-992, cucm_decompress_v2.cu:898-903):
+ * the StateMaps and Mixer trained by the host prelearn pass (prelearn,
+ * cucm_compress_v2.cu:924-981), or zero.  Host memory (~450 MiB: the trained
+ * tables and their device image). */
+typedef struct cucm_model cucm_model;
+/* The model after the prelearn pass over prefix[0..n). */
+int cucm_model_prelearn(const uint8_t *prefix, uint64_t n, cucm_model **out);
+/* The model a container's prelearn block defines (its prefix decoded and
+ * replayed, cucm_decompress_v2.cu:1056-1182 and :1209-1219).  *out is NULL,
+ * with CUCM_OK, for a container without a prelearn block. */
+int cucm_model_from_container(const uint8_t *in, uint64_t n, cucm_model **out);
+int cucm_model_destroy(cucm_model *m);
+/* cucm_compress_batch / cucm_decompress_batch starting every chunk from `m`
+ * (sm_init / mixer_init); m = NULL is the zero model.  The batch bodies of a
+ * prelearned container are exactly these with the container's model. */
+int cucm_compress_batch_model(cucm_ctx *ctx, const uint8_t *in, uint64_t n, uint64_t chunksize, uint32_t unit,
+                              const cucm_model *m, uint8_t *out, uint64_t cap, uint64_t *out_n);
+int cucm_decompress_batch_model(cucm_ctx *ctx, const uint8_t *body, uint64_t body_n, uint64_t chunksize,
+                                uint32_t unit, const cucm_model *m, uint8_t *out, uint64_t out_n);
+
+/* Multi-GPU building blocks (no counterpart in the reference, which codes on
+ * one GPU).  Chunks are independent, so the chunks of one stream can be coded
+ * on several GPUs and joined afterwards.
+ *
+ * cucm_compress_batch_dev: cucm_compress_batch_model with device buffers. */
+int cucm_compress_batch_dev(cucm_ctx *ctx, const uint8_t *d_in, uint64_t n, uint64_t chunksize, uint32_t unit,
+                            const cucm_model *m, uint8_t *d_out, uint64_t cap, uint64_t *out_n);
+/* Join batch bodies into one container.  Body i holds counts[i] consecutive
+ * chunks of the stream (what cucm_compress_batch returns for them: big-endian
+ * end offsets, then payloads), the bodies in stream order; p gives chunk
+ * size, unit and batch (prelearn 0), orig_size the stream's bytes.  The
+ * result is byte-identical to cucm_compress of the whole stream.  Host
+ * buffers and no device work; the _dev form reads device bodies and writes
+ * a device container on ctx's GPU. */
+int cucm_frame_bodies(const cucm_params *p, uint64_t orig_size, uint32_t nbodies, const uint8_t *const *bodies,
+                      const uint64_t *body_ns, const uint32_t *counts, uint8_t *out, uint64_t cap,
+                      uint64_t *out_n);
+int cucm_frame_bodies_dev(cucm_ctx *ctx, const cucm_params *p, uint64_t orig_size, uint32_t nbodies,
+                          const uint8_t *const *bodies, const uint64_t *body_ns, const uint32_t *counts,
+                          uint8_t *d_out, uint64_t cap, uint64_t *out_n);
+/* Decode chunks [first, first + count) of a container held in device memory
+ * into d_out (count chunks of the chunk size, the stream's last one
+ * possibly shorter); *out_n is that byte count. */
+int cucm_decompress_range_dev(cucm_ctx *ctx, const uint8_t *d_in, uint64_t n, uint64_t first, uint64_t count,
+                              uint8_t *d_out, uint64_t cap, uint64_t *out_n);
 
 /* Many independent containers in one call: the batched form.  Entry i
  * reads ins[i][0..ns[i]) and writes outs[i] (caps[i] bytes), its size to

@@ -92,3 +92,36 @@ def test_tuning_layout_and_autotune_arguments(cucm_lib):
     assert cucm_lib.cucm_autotune(None, buf, 16, ctypes.byref(p), 1, None, 0, ctypes.byref(n), ctypes.byref(t)) == -1
     # a null result array with a nonzero capacity is refused before any device work
     assert cucm_lib.cucm_autotune(None, buf, 16, ctypes.byref(p), 1, None, 4, ctypes.byref(n), ctypes.byref(t)) == -1
+
+
+def test_model_from_container_host_side(cucm_lib):
+    """The prelearn model is host work (no GPU): a container without a
+    prelearn block has no model, a malformed header is refused."""
+    gold = os.path.join(ROOT, "tests", "golden")
+    with open(os.path.join(gold, "text_20k_cs4k.cucm"), "rb") as f:
+        plain = f.read()
+    h = ctypes.c_void_p()
+    assert cucm_lib.cucm_model_from_container(plain, len(plain), ctypes.byref(h)) == 0 and not h.value
+    assert cucm_lib.cucm_model_from_container(plain, 10, ctypes.byref(h)) == -3
+    assert cucm_lib.cucm_model_destroy(None) == -1
+    with open(os.path.join(gold, "text_12k_pre3000.cucm"), "rb") as f:
+        pre = f.read()
+    m = cucm_b200.Model.from_container(pre)
+    assert m is not None
+    m.close()
+    m = cucm_b200.Model.prelearn(b"some prefix bytes" * 10)
+    m.close()
+
+
+def test_frame_bodies_argument_checks(cucm_lib):
+    p = cucm_b200.default_params(chunksize=4096)
+    got = ctypes.c_uint64()
+    # chunk counts that do not add up to the stream's chunks
+    body = (ctypes.c_void_p * 1)(None)
+    ns = (ctypes.c_uint64 * 1)(0)
+    cs = (ctypes.c_uint32 * 1)(2)
+    assert cucm_lib.cucm_frame_bodies(ctypes.byref(p), 4096, 1, body, ns, cs, None, 0, ctypes.byref(got)) == -1
+    # the empty stream: header only
+    out = ctypes.create_string_buffer(64)
+    assert cucm_lib.cucm_frame_bodies(ctypes.byref(p), 0, 0, None, None, None, out, 64, ctypes.byref(got)) == 0
+    assert got.value == 21

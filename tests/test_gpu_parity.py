@@ -123,3 +123,26 @@ def test_bad_container_rejected(gpu_ctx):
     blob = bytearray(gpu_ctx.compress(b"hello world" * 100, chunksize=256))
     with pytest.raises(cc.CucmError):
         gpu_ctx.decompress(bytes(blob[:30]))
+
+
+@pytest.mark.parametrize("name", ["text_12k_pre3000", "random_12k_pre2000"])
+def test_batch_bodies_of_prelearned_container(gpu_ctx, name):
+    """compress_batch / decompressbatch with the reference's sm_init and
+    mixer_init: a prelearned container's batch body is the batch coded from
+    the container's model, and decodes back through it."""
+    gpu_ctx.set_tuning(form=cc.FORM_PERSISTENT)
+    entry = next(e for e in MANIFEST if e["name"] == name)
+    data = make_input(entry)
+    with open(os.path.join(GOLDEN, name + ".cucm"), "rb") as f:
+        golden = f.read()
+    pre = entry["prelearn"]
+    coded = int.from_bytes(golden[12:16], "big")
+    pl_len = coded if golden[20] else pre
+    at = 21 + pl_len
+    body = golden[at + 4:at + 4 + int.from_bytes(golden[at:at + 4], "little")]
+    rest = data[pre:]
+    for model in (cc.Model.from_container(golden), cc.Model.prelearn(data[:pre])):
+        assert gpu_ctx.compress_batch(rest, entry["chunksize"], entry["unit"], model=model) == body
+        assert gpu_ctx.decompressbatch(body, len(rest), entry["chunksize"], entry["unit"], model=model) == rest
+    # the zero model gives a different body for the same bytes
+    assert gpu_ctx.compress_batch(rest, entry["chunksize"], entry["unit"]) != body
