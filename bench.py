@@ -13,6 +13,14 @@ is larger than L2, so no flush is needed between steps.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload mixed256M|batch|serve|small]
 
+The headline line also carries, unless --no-extras: "batched_vs_plain" (the
+4096-buffer set, batched persistent form against the plain form on a
+stratified 512-buffer sample, every batched container hashed against the
+reference's) and "serve" (the serving loop at offered loads of 2, 8 and
+32 GB/s, 32 requests each, p50/p99 latency and sustained MB/s against one
+request at a time).  "sha256_match" compares the timed workload's container
+with the reference's.
+
 Other workloads (one JSON line each, not the headline):
   batch  -- 4096 independent buffers, log-uniform 4 KiB..4 MiB, 256 KiB chunks:
             the batched persistent form (one launch for all buffers) against
@@ -27,10 +35,12 @@ host cores: its two programs built for the CPU from its unmodified sources
 (oracle/_ref), one chunk per process on all cores, on a bounded sample of
 the same workload.  Under torchrun, rank 0 alone runs it.
 
-Multi-GPU: one process per GPU; each rank codes its own copy of the
-workload (chunks are independent, there is no data-path exchange), so the
-scaling is weak; the timed region is bracketed by barriers and the slowest
-rank's device time is used.
+Multi-GPU (--gpus N; started under torchrun by the script itself when run
+alone): one process per GPU, one stream of N x 256 MiB split into
+contiguous chunk ranges, one per rank (cucm_b200/sharded.py).  The chunk
+bodies are gathered to rank 0 and framed into one container; rank 0
+broadcasts it, every rank decodes its range and the bytes go back to rank 0.
+Weak scaling; the slowest rank's time is used.
 """
 import argparse
 import json
@@ -65,6 +75,10 @@ def parse():
                          "32 MiB sample cut into the same 256 chunks)")
     ap.add_argument("--plain-sample", type=int, default=512, help="buffers the plain form codes (batch)")
     ap.add_argument("--requests", type=int, default=48, help="requests per offered load (serve)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="mixed256M: leave out the batched-vs-plain and serving figures of the headline line")
+    ap.add_argument("--extra-requests", type=int, default=32,
+                    help="requests per offered load of the headline line's serving figures")
     ap.add_argument("--loads", default="0.02,0.2,2,8,32", help="offered loads in GB/s (serve)")
     ap.add_argument("--small-bytes", type=int, default=1 << 20, help="bytes of the small workload")
     ap.add_argument("--small-source", default="text", choices=["text", "mixed"],
@@ -283,9 +297,120 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def relaunch_under_torchrun(args):
+    """`--gpus N` outside torchrun: start the N ranks (one per GPU) by
+    running this script again under torch.distributed.run on this node."""
+    import socket
+    with socket.socket() as s_:
+        s_.bind(("127.0.0.1", 0))
+        port = s_.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % args.gpus,
+           "--master-addr=127.0.0.1", "--master-port=%d" % port, os.path.abspath(__file__)] + sys.argv[1:]
+    os.execv(sys.executable, cmd)
+
+
+def run_sharded(args, rank, world, local):
+    """N GPUs, one rank each: one stream of N x 256 MiB whose N blocks are
+    the 256 MiB mixed buffer, 1 MiB chunks.  Each rank owns a contiguous range
+    of 256 chunks.  Compress: every rank codes its range, the body sizes are
+    all-gathered and the bodies sent to rank 0 (NCCL), which frames the
+    container.  Decompress: rank 0 broadcasts the container, every rank
+    decodes its range and sends it back.  Weak scaling; each phase is timed
+    with CUDA events (exchanges included), synchronised on both sides, and
+    the slowest rank's time is used."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import cucm_b200 as cc
+    from cucm_b200 import sharded
+    from cucm_b200 import workloads as W
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    data, _ = W.config1()
+    n = data.size
+    total = n * world
+    cs, unit, batch = PARAMS["chunksize"], PARAMS["unit"], PARAMS["batch"]
+    assert sharded.split_chunks(total // cs, world)[rank] == (rank * (n // cs), n // cs)
+    ctx = cc.Context(local)
+    coder = sharded.DeviceCoder(ctx, dev)
+    d_in = torch.from_numpy(data).to(dev)
+    h_in = torch.from_numpy(data).pin_memory()
+    h_out = torch.empty(total, dtype=torch.uint8).pin_memory() if rank == 0 else None
+
+    def step(host):
+        torch.cuda.synchronize()
+        dist.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        block = d_in
+        if host:
+            block = torch.empty_like(d_in)
+            block.copy_(h_in, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+        cont = sharded.compress_sharded(coder, block, total, cs, unit, batch, dist=dist)
+        ev[1].record()
+        back = sharded.decompress_sharded(coder, cont, total, cs, dist=dist)
+        if host and rank == 0:
+            h_out.copy_(back, non_blocking=True)
+        ev[2].record()
+        torch.cuda.synchronize()
+        return cont, back, ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+
+    ok = True
+    cont = None
+    for _ in range(max(args.warmup, 1)):
+        cont, back, _, _ = step(False)
+        if rank == 0:
+            ok = ok and all(torch.equal(back[r * n:(r + 1) * n], d_in) for r in range(world))
+    comp_n = cont.numel() if rank == 0 else 0
+    sampler = ClockSampler(local)
+    sampler.start()
+    tc = td = 0.0
+    for _ in range(args.steps):
+        _, _, a, b = step(False)
+        tc += a
+        td += b
+    clocks = sampler.stop()
+    t_all, t_c, t_d = reduce_max([tc + td, tc, td], dist, dev)
+    e_ms = 0.0
+    for i in range(args.steps + 1):
+        _, _, a, b = step(True)
+        if i:
+            e_ms += a + b
+    if rank == 0:
+        ok = ok and all(torch.equal(h_out[r * n:(r + 1) * n], h_in) for r in range(world))
+    e_max = reduce_max([e_ms], dist, dev)[0]
+    K = max(args.steps, 1)
+    if rank == 0:
+        line = {
+            "metric": "compress+decompress round-trip MB/s", "value": total * K / (t_all / 1e3) / 1e6,
+            "unit": "MB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_all / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "one stream of %d x 256 MiB (the mixed buffer per rank), 1 MiB chunks, unit 128, "
+                                   "batch 100" % world, "chunksize": cs, "unit": unit, "batch": batch,
+                       "parallelism": "contiguous chunk ranges per rank; bodies gathered and framed on rank 0, "
+                                      "container broadcast, ranges decoded per rank and gathered (NCCL)",
+                       "l2": "inputs larger than L2"},
+            "compress_MBps": total * K / (t_c / 1e3) / 1e6, "decompress_MBps": total * K / (t_d / 1e3) / 1e6,
+            "compressed_bytes": int(comp_n), "byte_exact": bool(ok),
+            "e2e": {"value": total * K / (e_max / 1e3) / 1e6, "unit": "MB/s", "h2d_bytes_per_step": total,
+                    "d2h_bytes_per_step": total},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    if not ok:
+        raise SystemExit("sharded round trip mismatch")
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        relaunch_under_torchrun(args)
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -293,17 +418,15 @@ def main():
         if rank == 0:
             {"batch": run_batch, "serve": run_serve, "small": run_small}[args.workload](args)
         return
+    if world > 1:
+        run_sharded(args, rank, world, local)
+        return
     import numpy as np
     import torch
     import cucm_b200 as cc
     from cucm_b200 import workloads as W
 
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = None  # the single-GPU path; N > 1 runs run_sharded
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
@@ -442,6 +565,14 @@ def main():
     }
     if tuned:
         line["autotune"] = tuned
+    if world == 1 and not args.no_extras:
+        # configs 2-4 beside the headline: the device is handed over whole
+        ctx.close()
+        del d_in, d_comp, d_dec
+        torch.cuda.empty_cache()
+        line["batched_vs_plain"] = batch_measure(warmup=1, sample=512)
+        torch.cuda.empty_cache()
+        line["serve"] = serve_measure([2.0, 8.0, 32.0], args.extra_requests)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -489,9 +620,13 @@ def run_small(args):
         raise SystemExit("round trip mismatch")
 
 
-def run_batch(args):
-    """Config 2 / 3: 4096 buffers, batched persistent form vs plain form."""
-    import numpy as np
+def batch_measure(warmup=1, sample=512):
+    """Configs 2 / 3: the 4096 buffers, batched persistent form (one launch
+    for every chunk of every buffer) against the plain form (one launch per
+    chunk) on a stratified sample of `sample` buffers (every n/k-th buffer in
+    size order, smallest and largest included), device buffers, plus every
+    batched container hashed against the reference's."""
+    import hashlib
     import torch
     import cucm_b200 as cc
     from cucm_b200 import workloads as W
@@ -518,46 +653,49 @@ def run_batch(args):
         if any(st2):
             raise SystemExit("decompress_many_dev failed: %s" % sorted(set(st2)))
         ok = all(torch.equal(x[:len(b)], y[:len(b)]) for x, y, b in zip(back, d_in, sub))
-        blobs = [bytes(x[:m].cpu().numpy().tobytes()) for x, m in zip(d_out, sizes)]
+        digests = [hashlib.sha256(x[:m].cpu().numpy().tobytes()).hexdigest() for x, m in zip(d_out, sizes)]
         nb = sum(len(b) for b in sub)
-        return dict(bytes=nb, compressed=sum(sizes), compress_ms=sc["device_ms"], decompress_ms=sd["device_ms"],
-                    compress_launches=sc["launches"], decompress_launches=sd["launches"],
-                    compress_MBps=_mbps(nb, sc["device_ms"]), decompress_MBps=_mbps(nb, sd["device_ms"]),
-                    round_trip_MBps=_mbps(nb, sc["device_ms"] + sd["device_ms"]), roundtrip_ok=ok), blobs
+        del d_in, d_out, back
+        return dict(buffers=len(sub), bytes=nb, compressed=sum(sizes), compress_ms=sc["device_ms"],
+                    decompress_ms=sd["device_ms"], compress_launches=sc["launches"],
+                    decompress_launches=sd["launches"], compress_MBps=_mbps(nb, sc["device_ms"]),
+                    decompress_MBps=_mbps(nb, sd["device_ms"]),
+                    round_trip_MBps=_mbps(nb, sc["device_ms"] + sd["device_ms"]), roundtrip_ok=ok), digests
 
-    for _ in range(max(args.warmup, 0)):
+    for _ in range(max(warmup, 0)):
         dev_round(bufs[:64], cc.FORM_PERSISTENT)
-    sub = bufs[:args.plain_sample]
-    plain, blobs_p = dev_round(sub, cc.FORM_PLAIN)
-    batched_sub, blobs_b = dev_round(sub, cc.FORM_PERSISTENT)
-    full, _ = dev_round(bufs, cc.FORM_PERSISTENT)
-    same = blobs_p == blobs_b
-    # end to end through the host-buffer batched API (pinned inputs)
-    pinned = [torch.from_numpy(b).pin_memory().numpy() if len(b) else b for b in bufs]
-    ctx.set_tuning(form=cc.FORM_PERSISTENT)
-    t0 = time.perf_counter()
-    blobs_h = ctx.compress_many(pinned, **p)
-    e_c = ctx.last_stats()["device_ms"]
-    back_h = ctx.decompress_many(blobs_h)
-    e_d = ctx.last_stats()["device_ms"]
-    wall = time.perf_counter() - t0
-    e2e_ok = all(x == y.tobytes() for x, y in zip(back_h, bufs))
-    nfull = full["bytes"]
-    line = {
-        "metric": "batched compress+decompress round-trip MB/s", "value": full["round_trip_MBps"], "unit": "MB/s",
-        "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "4096 buffers, log-uniform 4 KiB..4 MiB (%.2f GiB), 0.5 text / 0.25 walk / "
-                               "0.15 random / 0.1 runs, 256 KiB chunks, unit 128" % (nfull / 2**30),
-                   "form": "persistent (one launch for all buffers)"},
+    pick = W.config2_sample(sample)
+    sub = [bufs[i] for i in pick]
+    plain, dig_p = dev_round(sub, cc.FORM_PLAIN)
+    batched_sub, dig_b = dev_round(sub, cc.FORM_PERSISTENT)
+    full, dig_full = dev_round(bufs, cc.FORM_PERSISTENT)
+    ref = reference_sha256("many4096")
+    sha_ok = (dig_full == ref) if ref else None
+    ctx.close()
+    return {
+        "workload": "4096 buffers, log-uniform 4 KiB..4 MiB (%.2f GiB), 0.5 text / 0.25 walk / 0.15 random / "
+                    "0.1 runs, 256 KiB chunks, unit 128, device buffers" % (full["bytes"] / 2**30),
         "batched": full,
-        "plain_sample": {"buffers": len(sub), "plain": plain, "batched": batched_sub,
+        "plain_sample": {"sample": "%d buffers, every %d-th in size order (smallest and largest included)"
+                                   % (len(pick), len(bufs) // sample),
+                         "plain": plain, "batched": batched_sub,
                          "speedup_compress": batched_sub["compress_MBps"] / plain["compress_MBps"],
                          "speedup_decompress": batched_sub["decompress_MBps"] / plain["decompress_MBps"],
-                         "byte_identical": same},
-        "e2e": {"value": _mbps(nfull, e_c + e_d), "unit": "MB/s", "wall_s": wall, "roundtrip_ok": e2e_ok,
-                "h2d_bytes_per_step": nfull + full["compressed"], "d2h_bytes_per_step": nfull + full["compressed"]},
-        "byte_exact": bool(full["roundtrip_ok"] and plain["roundtrip_ok"] and same and e2e_ok),
+                         "speedup_round_trip": batched_sub["round_trip_MBps"] / plain["round_trip_MBps"],
+                         "byte_identical": dig_p == dig_b},
+        "sha256_match": sha_ok,
+        "byte_exact": bool(full["roundtrip_ok"] and plain["roundtrip_ok"] and batched_sub["roundtrip_ok"]
+                           and dig_p == dig_b and sha_ok is not False),
     }
+
+
+def run_batch(args):
+    """Configs 2 / 3 as a line of their own."""
+    r = batch_measure(args.warmup, args.plain_sample)
+    line = {"metric": "batched compress+decompress round-trip MB/s", "value": r["batched"]["round_trip_MBps"],
+            "unit": "MB/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": r["workload"], "form": "persistent (one launch for all buffers)"}}
+    line.update(r)
     print(json.dumps(line), flush=True)
 
 
@@ -566,20 +704,20 @@ def _pctl(xs, q):
     return float(np.percentile(np.asarray(xs), q)) if xs else None
 
 
-def run_serve(args):
-    """Config 4: the serving loop against one-request-at-a-time serving.  The
-    per-request form runs first on a context of its own, which is then
-    released, so that the server alone holds its HBM budget."""
+def serve_measure(loads, requests):
+    """Config 4: the serving loop under Poisson request streams at the given
+    offered loads (GB/s), against serving the same stream one request at a
+    time through the single-call API.  The per-request form runs first on a
+    context of its own, which is then released, so that the server alone
+    holds its HBM budget (120 GB)."""
     import numpy as np
     import torch
     import cucm_b200 as cc
     from cucm_b200 import workloads as W
-    loads = [float(x) for x in args.loads.split(",")]
     ctx = cc.Context(0)
     streams = []
     for li, gbps in enumerate(loads):
-        arrivals, comp, bufs, p = W.config4(args.requests, gbps, seed=4 + li)
-        cs = p["chunksize"]
+        arrivals, comp, bufs, p = W.config4(requests, gbps, seed=4 + li)
         dec_idx = [i for i in range(len(bufs)) if not comp[i]]
         blobs = ctx.compress_many([bufs[i] for i in dec_idx], **p) if dec_idx else []
         inputs = []
@@ -634,16 +772,22 @@ def run_serve(args):
                         "byte_exact": bool(exact)})
     info = srv.stats()
     srv.close()
-    best = max(r["serve"]["sustained_MBps"] for r in results)
-    print(json.dumps({"metric": "serving sustained MB/s and p50/p99 latency", "value": best, "unit": "MB/s",
-                      "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic",
-                      "config": {"workload": "Poisson request streams, %d requests per load, sizes log-uniform "
-                                             "1 KiB..16 MiB, 70%% compress / 30%% decompress, content as the "
-                                             "4096-buffer set, 256 KiB chunks, HBM budget 120 GB"
-                                             % args.requests,
-                                 "slots": info["slots"]},
-                      "levels": results,
-                      "byte_exact": all(r["byte_exact"] for r in results)}), flush=True)
+    return {"workload": "Poisson request streams, %d requests per load, sizes log-uniform 1 KiB..16 MiB, "
+                        "70%% compress / 30%% decompress, content as the 4096-buffer set, 256 KiB chunks, "
+                        "HBM budget 120 GB; latency from submit to result on the host" % requests,
+            "slots": info["slots"], "levels": results,
+            "byte_exact": all(r["byte_exact"] for r in results)}
+
+
+def run_serve(args):
+    """Config 4 as a line of its own."""
+    r = serve_measure([float(x) for x in args.loads.split(",")], args.requests)
+    best = max(x["serve"]["sustained_MBps"] for x in r["levels"])
+    line = {"metric": "serving sustained MB/s and p50/p99 latency", "value": best, "unit": "MB/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": r["workload"], "slots": r["slots"]}}
+    line.update(r)
+    print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":
