@@ -51,7 +51,7 @@ struct cucm_ctx {
   uint32_t nslots = 0;
   DevBuf image;    // prelearned slot image (when used)
   DevBuf d_init;   // ModelInit
-  DevBuf d_tasks, d_results, d_queue, d_status, d_scratch, d_big, d_pack, d_body, d_out;
+  DevBuf d_tasks, d_results, d_queue, d_status, d_scratch, d_big, d_pack, d_body, d_out, d_tails;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around the engine launches
   double last_ms = 0.0;
@@ -217,8 +217,14 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
     if (rc) return rc;
     CK(c->d_tasks.ensure(sizeof(ChunkTask) * n));
     CK(cudaMemcpyAsync(c->d_tasks.p, tasks.data(), sizeof(ChunkTask) * n, cudaMemcpyHostToDevice, c->stream));
-    CK(c->d_queue.ensure(sizeof(uint32_t)));
-    CK(cudaMemsetAsync(c->d_queue.p, 0, sizeof(uint32_t), c->stream));
+    // work-queue counter and tail-task counter, then the tail tasks
+    CK(c->d_queue.ensure(2 * sizeof(uint32_t)));
+    CK(cudaMemsetAsync(c->d_queue.p, 0, 2 * sizeof(uint32_t), c->stream));
+    TailTask *tails = nullptr;
+    if (!decode) {
+      CK(c->d_tails.ensure(sizeof(TailTask) * n));
+      tails = c->d_tails.as<TailTask>();
+    }
     const uint8_t *img = ms.image ? c->image.as<uint8_t>() : nullptr;
     CK(cudaEventRecord(c->evk0, c->stream));
     cudaError_t e = decode ? launch_decompress(c->d_tasks.as<ChunkTask>(), n, c->slots.as<uint8_t>(), grid, img,
@@ -226,11 +232,12 @@ int run_engine(cucm_ctx *c, bool decode, std::vector<ChunkTask> &tasks, int unit
                                                c->d_status.as<uint32_t>(), cfg, c->stream, unit)
                            : launch_compress(c->d_tasks.as<ChunkTask>(), n, c->slots.as<uint8_t>(), grid, img,
                                              c->d_init.as<ModelInit>(), c->d_queue.as<uint32_t>(),
-                                             c->d_status.as<uint32_t>(), cfg, c->stream, unit);
+                                             c->d_status.as<uint32_t>(), cfg, c->stream, unit, tails,
+                                             c->d_queue.as<uint32_t>() + 1);
     CK(e);
     CK(cudaEventRecord(c->evk1, c->stream));
     c->kernel_pending = true;
-    c->launches += 1;
+    c->launches += decode ? 1 : 2;  // the compressor's tail pass follows its engine launch
   } else {
     // Plain form: one single-CTA launch per chunk.  At most 128 grids can be
     // resident on the device, so chunks are spread over <= 128 streams, each

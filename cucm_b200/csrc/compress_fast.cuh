@@ -41,6 +41,17 @@ constexpr int kFrontThreads = 128;
 constexpr int kSnapThreads = 32 + kFrontThreads;  // chain + front warps
 constexpr int kWinBytes = kFastMaxUnit / 8 + 8;    // input window of a unit (+7 history bytes)
 
+constexpr int kFastStageMin = 2048;
+
+// The tables a compress CTA keeps in shared memory: the adaptation rates of
+// the chain and the state machine of the walker.  Stretch and squash are read
+// through the read-only cache from the device copy instead, which the SM's
+// CTAs share: that is what lets three CTAs share an SM at units <= 128.
+struct FastTables {
+  uint16_t dt[1024];
+  uint8_t nex[256][2];
+};
+
 struct FastLayout {
   int U, NSLOT, NBK, logNBK, stage;
   size_t off_tab, off_rec, off_snap, off_w, off_hk, off_ns, off_key, off_lnk, off_bkt, off_fsw, off_st, off_fr,
@@ -53,8 +64,8 @@ __host__ __device__ inline FastLayout make_fast_layout(int U) {
   L.NSLOT = next_pow2(2 * U);   // hash slots per order and unit (load <= 1/2)
   L.NBK = L.NSLOT / 4;          // 4-slot buckets, one 16-byte load each
   L.logNBK = ilog2(L.NBK);
-  L.stage = next_pow2(4 * U + 1024);
-  if (L.stage < kStageMin) L.stage = kStageMin;
+  L.stage = next_pow2(4 * U + 1024);  // a unit codes at most 4U bytes; flushes go out in 512-byte blocks
+  if (L.stage < kFastStageMin) L.stage = kFastStageMin;
   const size_t NS = (size_t)L.NSLOT;
   size_t o = 0;
   auto take = [&](size_t bytes) {
@@ -62,9 +73,9 @@ __host__ __device__ inline FastLayout make_fast_layout(int U) {
     o = (o + bytes + 15) & ~(size_t)15;
     return at;
   };
-  L.off_tab = take(sizeof(Tables));
+  L.off_tab = take(sizeof(FastTables));
   L.off_rec = take(sizeof(uint64_t) * kOrders * 256);
-  L.off_snap = take(sizeof(uint32_t) * kOrders * 256);
+  L.off_snap = take(sizeof(int16_t) * kOrders * 256);
   L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);
   L.off_hk = take(sizeof(uint32_t) * 2 * kOrders * NS);    // slot keys + 1, [unit parity][order][slot]
   L.off_ns = take(sizeof(uint16_t) * 2 * kOrders * NS);    // 0x100 | state once written in the unit
@@ -84,9 +95,9 @@ __host__ __device__ inline FastLayout make_fast_layout(int U) {
 }
 
 struct FastSmem {
-  Tables *tab;
+  FastTables *tab;
   uint64_t *rec;     // [256][8]  statep | dt[count] << 32 | dt[count + 1] << 48
-  uint32_t *snap;    // [256][8]  statep as of the last finished chain
+  int16_t *snap;     // [256][8]  stretched probability as of the last finished chain
   int32_t *w;        // [80*8]
   uint32_t *hk;      // [2][8][NSLOT]
   uint16_t *ns;      // [2][8][NSLOT]
@@ -105,9 +116,9 @@ struct FastSmem {
 
 __device__ inline FastSmem carve_fast(uint8_t *b, const FastLayout &L) {
   FastSmem s;
-  s.tab = reinterpret_cast<Tables *>(b + L.off_tab);
+  s.tab = reinterpret_cast<FastTables *>(b + L.off_tab);
   s.rec = reinterpret_cast<uint64_t *>(b + L.off_rec);
-  s.snap = reinterpret_cast<uint32_t *>(b + L.off_snap);
+  s.snap = reinterpret_cast<int16_t *>(b + L.off_snap);
   s.w = reinterpret_cast<int32_t *>(b + L.off_w);
   s.hk = reinterpret_cast<uint32_t *>(b + L.off_hk);
   s.ns = reinterpret_cast<uint16_t *>(b + L.off_ns);
@@ -123,6 +134,23 @@ __device__ inline FastSmem carve_fast(uint8_t *b, const FastLayout &L) {
   s.win = b + L.off_win;
   s.stage = b + L.off_stage;
   return s;
+}
+
+// Mixer output for one bit (Mixer::p, cucm_compress_v2.cu:636-644, then
+// `if (pr < 2048) pr++`), squash read through the read-only cache.
+__device__ __forceinline__ int mix_pr_ro(const int32_t *w, int cxt, const int smp[kOrders]) {
+  long long sum = 0;
+CUCM_UNROLL
+  for (int o = 0; o < kOrders; o++) sum += (long long)w[cxt * kOrders + o] * smp[o];
+  sum >>= 16;
+  const int idx = sum < -2047 ? -2047 : (sum > 2048 ? 2048 : (int)sum);
+  const int pr = __ldg(&g_tables.squash[idx + 2047]);
+  return pr < 2048 ? pr + 1 : pr;
+}
+
+__device__ inline void copy_fast_tables(FastTables *dst) {
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) dst->dt[i] = g_tables.dt[i];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) (&dst->nex[0][0])[i] = (&g_tables.nex[0][0])[i];
 }
 
 __device__ __forceinline__ void named_barrier(int id, int count) {
@@ -328,7 +356,7 @@ __device__ __forceinline__ void walk_unit(const FastSmem &s, const FastLayout &L
   uint16_t *ns_cur = s.ns + ((v & 1) * kOrders + o) * NS;
   const uint16_t *ns_prev = s.ns + (((v + 1) & 1) * kOrders + o) * NS;
   uint8_t *tab = slot + table_offset(o);
-  const Tables *tb = s.tab;
+  const FastTables *tb = s.tab;
   for (int q = 0; q < (n >> 3); q++) {
     const int ja = q * 8 + r0, jb = ja + 4;
     const int ia = ja * kOrders + o, ib = jb * kOrders + o;
@@ -430,7 +458,6 @@ __device__ __forceinline__ void front_mix(const FastSmem &s, const FastLayout &L
   const uint8_t *c1 = s.c1 + (v & 3) * (U / 8);
   uint16_t *prm = s.prm + (v & 1) * U;
   const uint16_t *prm_old = s.prm + ((v + 1) & 1) * U;
-  const Tables *tb = s.tab;
   int cxs[2] = {0, 0}, errs[2] = {0, 0};
   int smps[2][kOrders];
   bool has[2] = {false, false};
@@ -444,12 +471,12 @@ __device__ __forceinline__ void front_mix(const FastSmem &s, const FastLayout &L
         CUCM_UNROLL
         for (int o = 0; o < kOrders; o++) {
           const uint32_t stt = (uint32_t)(f8 >> (8 * o)) & 0xffu;
-          const int sm = tb->stretch[s.snap[stt * kOrders + o] >> 20];
+          const int sm = s.snap[stt * kOrders + o];
           smps[h][o] = sm;
           olen += (sm != 1);
         }
         const int cx = olen + (c1[j >> 3] >> 5) * 10;
-        const int pr = mix_pr(s.w, cx, smps[h], tb);
+        const int pr = mix_pr_ro(s.w, cx, smps[h]);
         const int y = (yw[j >> 5] >> (j & 31)) & 1;
         prm[j] = (uint16_t)((pr << 1) | y);
         cxs[h] = cx;
@@ -474,15 +501,15 @@ __device__ __forceinline__ void front_mix(const FastSmem &s, const FastLayout &L
 }
 
 // Front: table words holding the slot states of unit v, into registers.
-// Each thread takes entries e = t + 128 i (i < 16) of the [8][U] grid.
-constexpr int kGatherRegs = kOrders * kFastMaxUnit / kFrontThreads;  // 16
-
+// Each thread takes entries e = t + 128 i (i < GR) of the [8][U] grid; GR is
+// 8 for units up to 128 bits and 16 up to 256.
+template <int GR>
 __device__ __forceinline__ void front_gather(const FastSmem &s, const FastLayout &L, const uint8_t *slot, int t,
-                                             int v, int nvalid, uint32_t g[kGatherRegs]) {
+                                             int v, int nvalid, uint32_t g[GR]) {
   const int U = L.U;
   const uint32_t *key = s.key + (v & 1) * kOrders * U;
   CUCM_UNROLL
-  for (int i = 0; i < kGatherRegs; i++) {
+  for (int i = 0; i < GR; i++) {
     const int e = t + i * kFrontThreads;
     if (e < kOrders * U) {
       const int j = e >> 3, o = e & 7;
@@ -495,20 +522,24 @@ __device__ __forceinline__ void front_gather(const FastSmem &s, const FastLayout
   }
 }
 
+template <int GR>
 __device__ __forceinline__ void front_store_gather(const FastSmem &s, const FastLayout &L, int t, int v,
-                                                   const uint32_t g[kGatherRegs]) {
+                                                   const uint32_t g[GR]) {
   const int U = L.U;
   const uint32_t *key = s.key + (v & 1) * kOrders * U;
   uint8_t *fsb = s.fsw + (v & 1) * kOrders * U;
   CUCM_UNROLL
-  for (int i = 0; i < kGatherRegs; i++) {
+  for (int i = 0; i < GR; i++) {
     const int e = t + i * kFrontThreads;
     if (e < kOrders * U) fsb[e] = (uint8_t)(g[i] >> (8 * (key[e] & 3)));
   }
 }
 
+constexpr uint64_t kTailOffloadBits = 4096;  // shorter stale tails are coded in place
+
+template <int GR>
 __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastSmem &s, const FastLayout &L,
-                                  const ModelInit *init, uint32_t *status) {
+                                  const ModelInit *init, uint32_t *status, TailTask *tails, uint32_t *tail_count) {
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const int U = L.U;
@@ -533,7 +564,7 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
   for (int i = tid; i < 2 * kOrders * L.NSLOT; i += blockDim.x) s.hk[i] = 0;
 
   Coder c{0u, 0xffffffffu, 0, 0};
-  uint32_t g[kGatherRegs];
+  uint32_t g[GR];
   uint32_t wbyte = 0;
   __syncthreads();
 
@@ -547,8 +578,8 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
       front_sync();
     }
     front_links(s, L, ft, 0, fast_nvalid(data_bits, U, 0));
-    front_gather(s, L, slot, ft, 0, fast_nvalid(data_bits, U, 0), g);
-    front_store_gather(s, L, ft, 0, g);
+    front_gather<GR>(s, L, slot, ft, 0, fast_nvalid(data_bits, U, 0), g);
+    front_store_gather<GR>(s, L, ft, 0, g);
     if (nU > 2) wbyte = window_load(t.in, len, U, 2, ft);
   }
   __syncthreads();
@@ -557,11 +588,12 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
     const int um = tau - 1;
     // gathers of unit tau+1 go out first; they land while the front works
     const int nv1 = fast_nvalid(data_bits, U, tau + 1);
-    if (front && tau + 1 < nU) front_gather(s, L, slot, ft, tau + 1, nv1, g);
+    if (front && tau + 1 < nU) front_gather<GR>(s, L, slot, ft, tau + 1, nv1, g);
     if (warp == kWChain || front) {
       if (um >= 0 && um < nU) {
         const int k = warp == kWChain ? lane : 32 + ft;
-        for (int i = k; i < kOrders * 256; i += kSnapThreads) s.snap[i] = (uint32_t)s.rec[i];
+        for (int i = k; i < kOrders * 256; i += kSnapThreads)
+          s.snap[i] = __ldg(&g_tables.stretch[(uint32_t)s.rec[i] >> 20]);
       }
       named_barrier(1, kSnapThreads);
     }
@@ -590,7 +622,7 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
           front_keys(s, L, ft, tau + 2, fast_nvalid(data_bits, U, tau + 2));
           if (tau + 3 < nU) wbyte = window_load(t.in, len, U, tau + 3, ft);
         }
-        front_store_gather(s, L, ft, tau + 1, g);
+        front_store_gather<GR>(s, L, ft, tau + 1, g);
       }
     }
     __syncthreads();
@@ -598,26 +630,57 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
 
   if (warp == kWCoder) {
     const uint16_t *last = s.prm + ((nU - 1) & 1) * U;
-    for (int v = nU;; v++) {
-      const int n = ncode_of(v);
-      if (n <= 0) break;
-      coder_run_p(c, last, s.stage, L.stage, n);
-      coder_flush_p(c, s.stage, L.stage, t.out, t.out_cap);
+    const uint64_t coded = (uint64_t)nU * U;
+    const uint64_t left = total_bits > coded ? total_bits - coded : 0;
+    if (tails && left >= kTailOffloadBits) {
+      // the stale tail goes to the tail pass: the ring drains to the
+      // payload, the coder state and the unit buffer to a tail task, and the
+      // CTA moves on to its next chunk
+      const uint32_t mask = (uint32_t)L.stage - 1;
+      for (uint64_t i = c.flushed + lane; i < c.head; i += 32)
+        if (i < t.out_cap) t.out[i] = s.stage[(uint32_t)i & mask];
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(tail_count, 1u);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      TailTask &T = tails[k];
+      for (int j = lane; j < U; j += 32) T.prm[j] = last[j];
+      if (lane == 0) {
+        T.out = t.out;
+        T.cap = t.out_cap;
+        T.result = t.result;
+        T.head = c.head;
+        T.bits = left;
+        T.x1 = c.x1;
+        T.x2 = c.x2;
+        T.unit = (uint32_t)U;
+      }
+      __syncwarp();
+    } else {
+      for (int v = nU;; v++) {
+        const int n = ncode_of(v);
+        if (n <= 0) break;
+        coder_run_p(c, last, s.stage, L.stage, n);
+        coder_flush_p(c, s.stage, L.stage, t.out, t.out_cap);
+      }
+      coder_finish_p(c, s.stage, L.stage, t.out, t.out_cap, t.result);
+      if (lane == 0 && c.head > t.out_cap) atomicOr(status, (uint32_t)kDevOverflow);
     }
-    coder_finish_p(c, s.stage, L.stage, t.out, t.out_cap, t.result);
-    if (lane == 0 && c.head > t.out_cap) atomicOr(status, (uint32_t)kDevOverflow);
   }
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kFastThreads, 2)
-    compress_fast_kernel(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, const uint8_t *init_tables,
-                         const ModelInit *init, uint32_t *queue, uint32_t *status, int unit) {
+// Persistent CTA: chunks from the work queue, one after the other, each in
+// this CTA's slot tables (restored to the initial model between chunks).
+template <int GR>
+__device__ __forceinline__ void compress_fast_loop(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots,
+                                                   const uint8_t *init_tables, const ModelInit *init,
+                                                   uint32_t *queue, uint32_t *status, int unit, TailTask *tails,
+                                                   uint32_t *tail_count) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const FastLayout L = make_fast_layout(unit);
   const FastSmem s = carve_fast(smem_raw, L);
   uint8_t *slot = slots + (size_t)blockIdx.x * kSlotTableBytes;
-  copy_tables(&g_tables, s.tab);
+  copy_fast_tables(s.tab);
   __shared__ uint32_t s_task;
   bool fresh = true;
   for (;;) {
@@ -639,17 +702,79 @@ __global__ void __launch_bounds__(kFastThreads, 2)
       __syncthreads();
     }
     fresh = false;
-    compress_fast_one(t, slot, s, L, init, status);
+    compress_fast_one<GR>(t, slot, s, L, init, status, tails, tail_count);
   }
 }
 
-// One chunk, task passed by value, tables at `slot` (no work queue).
+// Units up to 128 bits: three CTAs share an SM (registers capped to fit).
+__global__ void __maxnreg__(96)
+    compress_fast_kernel(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, const uint8_t *init_tables,
+                         const ModelInit *init, uint32_t *queue, uint32_t *status, int unit, TailTask *tails,
+                         uint32_t *tail_count) {
+  compress_fast_loop<8>(tasks, ntasks, slots, init_tables, init, queue, status, unit, tails, tail_count);
+}
+
+// Units of 160..256 bits.
+__global__ void __launch_bounds__(kFastThreads, 2)
+    compress_fast_kernel_wide(const ChunkTask *tasks, uint32_t ntasks, uint8_t *slots, const uint8_t *init_tables,
+                              const ModelInit *init, uint32_t *queue, uint32_t *status, int unit, TailTask *tails,
+                              uint32_t *tail_count) {
+  compress_fast_loop<16>(tasks, ntasks, slots, init_tables, init, queue, status, unit, tails, tail_count);
+}
+
+// One chunk, task passed by value, tables at `slot` (no work queue); the
+// stale tail is coded in place.
+template <int GR>
 __global__ void __launch_bounds__(kFastThreads, 2)
     compress_fast_single_kernel(const ChunkTask t, uint8_t *slot, const ModelInit *init, uint32_t *status) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const FastLayout L = make_fast_layout((int)t.unit);
   const FastSmem s = carve_fast(smem_raw, L);
-  copy_tables(&g_tables, s.tab);
+  copy_fast_tables(s.tab);
   __syncthreads();
-  compress_fast_one(t, slot, s, L, init, status);
+  compress_fast_one<GR>(t, slot, s, L, init, status, nullptr, nullptr);
+}
+
+// The tail pass: one thread per handed-over chunk codes its stale tail (the
+// unit buffer again and again up to the chunk end), writes the bytes, the
+// flush byte (cucm_compress_v2.cu:902) and the payload length.  Same coder
+// step as coder_step; the buffer is read through the read-only cache, four
+// entries per load.
+__global__ void __launch_bounds__(128) compress_tail_kernel(const TailTask *tails, const uint32_t *count,
+                                                            uint32_t *status) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *count) return;
+  const TailTask &T = tails[i];
+  uint32_t x1 = T.x1, x2 = T.x2;
+  uint64_t head = T.head;
+  const uint64_t cap = T.cap;
+  uint8_t *out = T.out;
+  const uint32_t U = T.unit;
+  const uint64_t *prm4 = reinterpret_cast<const uint64_t *>(T.prm);
+  uint64_t left = T.bits;
+  uint32_t j4 = 0;  // next group of four entries
+  while (left) {
+    const uint64_t e4 = __ldg(prm4 + j4);
+    j4 = (4 * (j4 + 1) == U) ? 0u : j4 + 1;
+    const int n = left < 4 ? (int)left : 4;
+    left -= (uint64_t)n;
+CUCM_UNROLL
+    for (int q = 0; q < 4; q++) {
+      if (q < n) {
+        const uint32_t e = (uint32_t)(e4 >> (16 * q)) & 0xffffu;
+        const uint32_t xm = x1 + __umulhi(x2 - x1, (e >> 1) << 20);
+        if (e & 1) x2 = xm; else x1 = xm + 1;
+        while ((x1 ^ x2) < 0x1000000u) {
+          if (head < cap) out[head] = (uint8_t)(x2 >> 24);
+          head++;
+          x1 <<= 8;
+          x2 = (x2 << 8) | 255u;
+        }
+      }
+    }
+  }
+  if (head < cap) out[head] = (uint8_t)(x1 >> 24);
+  head++;
+  *T.result = head;
+  if (head > cap) atomicOr(status, (uint32_t)kDevOverflow);
 }

@@ -28,6 +28,22 @@ struct ChunkTask {
   uint64_t *result;      // compress: payload length written here (or > cap on overflow)
 };
 
+// The stale tail of a chunk handed from a persistent compress CTA to the tail
+// pass: the coder state after the chunk's last data unit, and the unit buffer
+// the reference keeps re-coding up to the chunk end
+// (cucm_compress_v2.cu:850-852).
+struct TailTask {
+  uint8_t *out;       // payload; bytes [0, head) are written
+  uint64_t cap;       // payload capacity
+  uint64_t *result;   // payload length goes here
+  uint64_t head;      // bytes produced so far
+  uint64_t bits;      // stale bits still to code: prm[j % unit] for j < bits
+  uint32_t x1, x2;
+  uint32_t unit;
+  uint32_t pad;
+  uint16_t prm[256];  // the last data unit's buffer (units up to 256 bits)
+};
+
 // Status words written by the kernels (per launch).
 enum DevStatus : uint32_t {
   kDevOk = 0,
@@ -53,9 +69,12 @@ cudaError_t upload_tables();  // once per device (current device)
 // slots: nslots chunk-slot tables of kSlotTableBytes each, already holding
 // the initial model states.  init_tables: a clean copy to restore slots from
 // between chunks (nullptr = restore to zero).  queue: one u32 counter.
+// tails: room for ntasks tail tasks and a zeroed u32 counter (tail_count),
+// or null to code every stale tail in place (the plain form passes null).
 cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                             const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
-                            uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit);
+                            uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit,
+                            TailTask *tails = nullptr, uint32_t *tail_count = nullptr);
 cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                               const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
                               uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit);

@@ -561,15 +561,37 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Pipelined compressor CTAs that fit on one SM: shared memory (1 KiB of it
+// reserved per CTA by the hardware) and, at units <= 128 bits, the 96-register
+// cap that lets three share the register file.
+static int fast_ctas_per_sm(int unit) {
+  const size_t per = make_fast_layout(unit).total + 1024 + 64;
+  const int by_smem = (int)((228u * 1024u) / per);
+  const int by_regs = unit <= 128 ? 3 : 2;
+  const int n = by_smem < by_regs ? by_smem : by_regs;
+  return n < 1 ? 1 : n;
+}
+
 cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                             const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
-                            uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit) {
+                            uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit,
+                            TailTask *tails, uint32_t *tail_count) {
   if (unit <= kFastMaxUnit && !cfg.generic) {
     const size_t smem = make_fast_layout(unit).total;
-    cudaError_t e = set_smem((const void *)compress_fast_kernel, smem);
+    const void *kern = unit <= 128 ? (const void *)compress_fast_kernel : (const void *)compress_fast_kernel_wide;
+    cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
-    compress_fast_kernel<<<nslots, kFastThreads, smem, stream>>>(d_tasks, ntasks, slots, init_tables, d_init,
-                                                                  d_queue, d_status, unit);
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    if (unit <= 128)
+      compress_fast_kernel<<<nslots, kFastThreads, smem, stream>>>(d_tasks, ntasks, slots, init_tables, d_init,
+                                                                    d_queue, d_status, unit, tails, tail_count);
+    else
+      compress_fast_kernel_wide<<<nslots, kFastThreads, smem, stream>>>(d_tasks, ntasks, slots, init_tables, d_init,
+                                                                         d_queue, d_status, unit, tails, tail_count);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !tails) return e;
+    compress_tail_kernel<<<(ntasks + 127) / 128, 128, 0, stream>>>(tails, tail_count, d_status);
     return cudaGetLastError();
   }
   const size_t smem = make_layout(unit, 0).total;
@@ -593,7 +615,10 @@ static bool dec_fast(int unit, const EngineConfig &cfg) { return unit <= kDecMax
 int engine_slots_per_sm(bool decode, int unit, const EngineConfig &cfg) {
   if (decode && dec_fast(unit, cfg))
     return cfg.dec_pairs > 0 ? std::min(cfg.dec_pairs, dec_max_pairs(unit)) : dec_max_pairs(unit);
-  if (!decode && unit <= kFastMaxUnit && !cfg.generic) return cfg.cmp_ctas == 1 ? 1 : 2;
+  if (!decode && unit <= kFastMaxUnit && !cfg.generic) {
+    const int fit = fast_ctas_per_sm(unit);
+    return cfg.cmp_ctas > 0 && cfg.cmp_ctas < fit ? cfg.cmp_ctas : fit;
+  }
   const size_t smem = decode ? decompress_smem_bytes(unit, cfg.spec_bits) : make_layout(unit, 0).total;
   return smem > 110 * 1024 ? 1 : (smem > 72 * 1024 ? 2 : 3);
 }

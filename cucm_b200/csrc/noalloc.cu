@@ -105,8 +105,11 @@ int noalloc_setup(int dev, NoAllocDevice *&out) {
   for (int i = 0; i < kMixCtx * kOrders; i++) zero.w[i] = 0;
   if (cudaMemcpyToSymbol(g_noalloc_init, &zero, sizeof zero) != cudaSuccess) return CUCM_ECUDA;
   const size_t smem = make_fast_layout(kFastMaxUnit).total;
-  if (cudaFuncSetAttribute((const void *)compress_fast_single_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute((const void *)compress_fast_single_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
+    return CUCM_ECUDA;
+  if (cudaFuncSetAttribute((const void *)compress_fast_single_kernel<16>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return CUCM_ECUDA;
   d.ready = true;
   return CUCM_OK;
@@ -138,7 +141,10 @@ extern "C" int cucm_compress_chunk_noalloc(const uint8_t *d_in, uint64_t len, ui
   t.unit = unit;
   t.result = d->result;
   const size_t smem = make_fast_layout((int)unit).total;
-  compress_fast_single_kernel<<<1, kFastThreads, smem, st>>>(t, d->slot, d->init, d->status);
+  if (unit <= 128)
+    compress_fast_single_kernel<8><<<1, kFastThreads, smem, st>>>(t, d->slot, d->init, d->status);
+  else
+    compress_fast_single_kernel<16><<<1, kFastThreads, smem, st>>>(t, d->slot, d->init, d->status);
   if (cudaGetLastError() != cudaSuccess) return CUCM_ECUDA;
   uint64_t got = 0;
   uint32_t status = 0;

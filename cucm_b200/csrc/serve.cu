@@ -96,7 +96,8 @@ struct Launch {
   std::vector<ChunkTask> tasks;  // in chunk order (not the launch order)
   uint8_t *d_in = nullptr, *d_scratch = nullptr, *d_out = nullptr, *d_image = nullptr;
   uint64_t *d_results = nullptr;
-  uint32_t *d_status = nullptr, *d_queue = nullptr;
+  uint32_t *d_status = nullptr, *d_queue = nullptr;  // d_queue[1]: tail-task counter
+  TailTask *d_tails = nullptr;                        // compress: stale tails for the tail pass
   ModelInit *d_init = nullptr;
   ChunkTask *d_tasks = nullptr;
   uint64_t *h_lens = nullptr;  // pinned
@@ -189,8 +190,9 @@ int prepare(Req *r) {
 // Device buffer bytes a request needs while it runs.
 uint64_t req_bytes(const Req *r) {
   const uint64_t pad = 256;
-  if (r->op == CUCM_OP_COMPRESS)  // input, scratch, packed output, tasks
-    return r->body_n + pad + r->nchunks * (2 * scratch_cap(r->cs) + sizeof(ChunkTask) + sizeof(PackEntry) + 24) +
+  if (r->op == CUCM_OP_COMPRESS)  // input, scratch, packed output, tasks, tail tasks
+    return r->body_n + pad +
+           r->nchunks * (2 * scratch_cap(r->cs) + sizeof(ChunkTask) + sizeof(PackEntry) + sizeof(TailTask) + 24) +
            4096;
   return r->body_n + pad + r->out_body + pad + r->nchunks * (sizeof(ChunkTask) + 16);
 }
@@ -289,7 +291,7 @@ int run_tasks(cucm_server *s, Launch *l, const std::vector<ChunkTask> &tasks) {
     return la > lb;
   });
   SCK(cudaMemcpyAsync(l->d_tasks, order.data(), sizeof(ChunkTask) * order.size(), cudaMemcpyHostToDevice, l->st));
-  SCK(cudaMemsetAsync(l->d_queue, 0, sizeof(uint32_t), l->st));
+  SCK(cudaMemsetAsync(l->d_queue, 0, 2 * sizeof(uint32_t), l->st));
   SCK(cudaMemsetAsync(l->d_status, 0, sizeof(uint32_t), l->st));
   const uint32_t grid = std::min<uint32_t>(l->nslot, (uint32_t)order.size());
   uint8_t *slots = s->slots + (size_t)l->slot0 * kSlotTableBytes;
@@ -297,7 +299,7 @@ int run_tasks(cucm_server *s, Launch *l, const std::vector<ChunkTask> &tasks) {
   cudaError_t e = dec ? launch_decompress(l->d_tasks, (uint32_t)order.size(), slots, grid, img, l->d_init, l->d_queue,
                                           l->d_status, cfg, l->st, (int)l->unit)
                       : launch_compress(l->d_tasks, (uint32_t)order.size(), slots, grid, img, l->d_init, l->d_queue,
-                                        l->d_status, cfg, l->st, (int)l->unit);
+                                        l->d_status, cfg, l->st, (int)l->unit, l->d_tails, l->d_queue + 1);
   SCK(e);
   s->launches++;
   return CUCM_OK;
@@ -360,6 +362,7 @@ int start_launch_in(cucm_server *s, Launch *l, std::vector<Req *> &grp, uint32_t
   l->d_in = (uint8_t *)dalloc(l, in_tot, &err);
   if (l->op == CUCM_OP_COMPRESS) {
     l->d_scratch = (uint8_t *)dalloc(l, nchunks * smax + 16, &err);
+    l->d_tails = (TailTask *)dalloc(l, sizeof(TailTask) * std::max<uint64_t>(nchunks, 1), &err);
     l->d_results = (uint64_t *)dalloc(l, 8 * std::max<uint64_t>(nchunks, 1), &err);
   } else {
     l->d_out = (uint8_t *)dalloc(l, out_tot, &err);
