@@ -39,9 +39,12 @@ class CucmError(RuntimeError):
         super().__init__("%s: %s (%s)" % (what or "cucm", msg, _ERRORS.get(status, status)))
 
 
+FORMAT_AUTO, FORMAT_32, FORMAT_64 = 0, 1, 2
+
+
 class Params(ctypes.Structure):
     _fields_ = [("chunksize", ctypes.c_uint64), ("unit", ctypes.c_uint32),
-                ("prelearn", ctypes.c_uint64), ("batch", ctypes.c_uint32)]
+                ("prelearn", ctypes.c_uint64), ("batch", ctypes.c_uint32), ("format", ctypes.c_uint32)]
 
 
 class Stats(ctypes.Structure):
@@ -170,9 +173,13 @@ def lib():
     return L
 
 
-def default_params(chunksize=None, unit=None, prelearn=None, batch=None):
+def default_params(chunksize=None, unit=None, prelearn=None, batch=None, fmt=None):
+    """cucm_params: the reference CLI's defaults, then the given fields; fmt
+    is the container format (FORMAT_AUTO, FORMAT_32 or FORMAT_64)."""
     p = Params()
     lib().cucm_default_params(ctypes.byref(p))
+    if fmt is not None:
+        p.format = int(fmt)
     if chunksize is not None:
         p.chunksize = int(chunksize)
     if unit is not None:
@@ -311,29 +318,46 @@ class Context:
                  for r in res[:min(count.value, 64)]]
         return _tuning_dict(best), cands
 
-    def compress(self, data, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
-        p = default_params(chunksize, unit, prelearn, batch)
+    def compress(self, data, chunksize=1 << 20, unit=128, prelearn=0, batch=100, fmt=FORMAT_AUTO, out=None):
+        """The container of `data`.  With `out` (a writable numpy uint8 array)
+        the container is written there and a view of it returned; otherwise
+        bytes, in a buffer of the compress bound."""
+        p = default_params(chunksize, unit, prelearn, batch, fmt)
         ptr, n, keep = _buf(data)
-        cap = lib().cucm_compress_bound(n, ctypes.byref(p))
-        out = ctypes.create_string_buffer(max(cap, 1))
         got = ctypes.c_uint64()
-        rc = lib().cucm_compress(self._h, ptr, n, ctypes.byref(p), out, cap, ctypes.byref(got))
+        if out is not None:
+            optr, cap, out = _buf_w(out)
+            rc = lib().cucm_compress(self._h, ptr, n, ctypes.byref(p), optr, cap, ctypes.byref(got))
+            if rc:
+                raise CucmError(rc, "cucm_compress")
+            return out[:got.value]
+        cap = lib().cucm_compress_bound(n, ctypes.byref(p))
+        buf = ctypes.create_string_buffer(max(cap, 1))
+        rc = lib().cucm_compress(self._h, ptr, n, ctypes.byref(p), buf, cap, ctypes.byref(got))
         if rc:
             raise CucmError(rc, "cucm_compress")
-        return out.raw[:got.value]
+        return buf.raw[:got.value]
 
-    def decompress(self, blob):
+    def decompress(self, blob, out=None):
+        """The original bytes of a container; into `out` (a writable numpy
+        uint8 array, returned as a view) when given."""
         ptr, n, keep = _buf(blob)
         size = ctypes.c_uint64()
         rc = lib().cucm_decompressed_size(ptr, n, ctypes.byref(size))
         if rc:
             raise CucmError(rc, "cucm_decompressed_size")
-        out = ctypes.create_string_buffer(max(size.value, 1))
         got = ctypes.c_uint64()
-        rc = lib().cucm_decompress(self._h, ptr, n, out, size.value, ctypes.byref(got))
+        if out is not None:
+            optr, cap, out = _buf_w(out)
+            rc = lib().cucm_decompress(self._h, ptr, n, optr, cap, ctypes.byref(got))
+            if rc:
+                raise CucmError(rc, "cucm_decompress")
+            return out[:got.value]
+        buf = ctypes.create_string_buffer(max(size.value, 1))
+        rc = lib().cucm_decompress(self._h, ptr, n, buf, size.value, ctypes.byref(got))
         if rc:
             raise CucmError(rc, "cucm_decompress")
-        return out.raw[:got.value]
+        return buf.raw[:got.value]
 
     def compress_dev(self, d_in, n, d_out, cap, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
         """Device pointers in and out; returns the container size."""
@@ -466,17 +490,17 @@ class Context:
         return dict(device_ms=st.device_ms, kernel_ms=st.kernel_ms, launches=st.launches, chunks=st.chunks)
 
 
-def frame_bodies(bodies, counts, orig_size, chunksize=1 << 20, unit=128, batch=100):
+def frame_bodies(bodies, counts, orig_size, chunksize=1 << 20, unit=128, batch=100, fmt=FORMAT_AUTO):
     """The container of a stream whose chunks were coded in consecutive
     pieces (cucm_frame_bodies; host buffers, no device work): bodies[i] is the
     batch body of counts[i] consecutive chunks."""
-    p = default_params(chunksize, unit, 0, batch)
+    p = default_params(chunksize, unit, 0, batch, fmt)
     k = len(bodies)
     bufs = [_buf(b) for b in bodies]
     ptrs = (ctypes.c_void_p * k)(*[b[0] for b in bufs])
     ns = (ctypes.c_uint64 * k)(*[b[1] for b in bufs])
     cs = (ctypes.c_uint32 * k)(*counts)
-    cap = 64 + 4 * ((sum(counts) + batch - 1) // batch) + sum(b[1] for b in bufs)
+    cap = 64 + 8 * ((sum(counts) + batch - 1) // batch) + 4 * sum(counts) + sum(b[1] for b in bufs)
     out = ctypes.create_string_buffer(cap)
     got = ctypes.c_uint64()
     rc = lib().cucm_frame_bodies(ctypes.byref(p), orig_size, k, ptrs, ns, cs, out, cap, ctypes.byref(got))

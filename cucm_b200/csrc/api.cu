@@ -370,9 +370,10 @@ int encode_chunks(cucm_ctx *c, const std::vector<Seg> &segs, uint64_t cs, uint32
 
 // Body layout of segment g's chunks (see layout_chunks).
 uint64_t layout_body(const Encoded &e, size_t g, uint32_t batch, bool with_sizes, uint8_t *base,
-                     std::vector<PackEntry> *pe) {
+                     std::vector<PackEntry> *pe, bool wide = false, bool *overflow = nullptr) {
   const uint64_t f = e.first[g];
-  return layout_chunks(e.lens.data() + f, e.src.data() + f, e.first[g + 1] - f, batch, with_sizes, base, pe);
+  return layout_chunks(e.lens.data() + f, e.src.data() + f, e.first[g + 1] - f, batch, with_sizes, base, pe, wide,
+                       overflow);
 }
 
 // One launch packs every laid-out body.
@@ -436,6 +437,7 @@ void cucm_default_params(cucm_params *p) {
   p->unit = 128;               // cucm_compress_v2.cu:1306
   p->prelearn = 0;
   p->batch = 100;              // cucm_compress_v2.cu:1312
+  p->format = CUCM_FORMAT_AUTO;
 }
 
 const char *cucm_strerror(int s) {
@@ -517,11 +519,18 @@ uint64_t cucm_compress_bound(uint64_t n, const cucm_params *p) {
   uint64_t body = n > p->prelearn ? n - p->prelearn : 0;
   uint64_t nchunks = (body + p->chunksize - 1) / p->chunksize;
   uint64_t nb = (nchunks + p->batch - 1) / p->batch;
-  return kHeaderBytes + p->prelearn * 8 + 8 + 4 * nb + nchunks * (4 + 32 * p->chunksize + 1);
+  const uint64_t fw = wide_format(p, n) ? 8 : 4;
+  const uint64_t hl = fw == 8 ? kHeaderBytes64 : kHeaderBytes;
+  return hl + p->prelearn * 8 + 8 + fw * nb + nchunks * (fw + 32 * p->chunksize + 1);
 }
 
 int cucm_decompressed_size(const uint8_t *in, uint64_t n, uint64_t *size) {
   if (!in || !size || n < 4) return CUCM_EFORMAT;
+  if (is_wide_header(in, n)) {
+    if (n < 16) return CUCM_EFORMAT;
+    *size = get_be64(in + 8);
+    return CUCM_OK;
+  }
   *size = get_be32(in);
   return CUCM_OK;
 }
@@ -604,9 +613,11 @@ static int compress_containers(cucm_ctx *c, uint32_t count, const uint8_t *const
     uint64_t stage = 0;
     for (size_t j = 0; j < grp.size(); j++) {
       const uint32_t i = grp[j];
-      body[j] = layout_body(e, j, p->batch, true, nullptr, nullptr);
+      bool overflow = false;
+      body[j] = layout_body(e, j, p->batch, true, nullptr, nullptr, wide_format(p, ns[i]), &overflow);
       out_ns[i] = hdrs[i].size() + body[j];
-      if (out_ns[i] > caps[i]) status[i] = CUCM_ENOSPC;
+      if (overflow) status[i] = CUCM_EINVAL;  // a batch past 4 GiB needs the 64-bit container
+      else if (out_ns[i] > caps[i]) status[i] = CUCM_ENOSPC;
       at[j] = stage;
       stage += (body[j] + 15) & ~15ull;
     }
@@ -616,7 +627,7 @@ static int compress_containers(cucm_ctx *c, uint32_t count, const uint8_t *const
       const uint32_t i = grp[j];
       if (status[i]) continue;
       uint8_t *base = dev ? outs[i] + hdrs[i].size() : c->d_out.as<uint8_t>() + at[j];
-      layout_body(e, j, p->batch, true, base, &pe);
+      layout_body(e, j, p->batch, true, base, &pe, wide_format(p, ns[i]));
     }
     rc = pack_bodies(c, pe);
     if (rc) break;
@@ -691,10 +702,11 @@ static int decompress_containers(cucm_ctx *c, uint32_t count, const uint8_t *con
       status[i] = CUCM_ENOSPC;
       continue;
     }
-    const uint64_t body_off = kHeaderBytes + ph[i].pl_len;
+    const uint64_t body_off = ph[i].body_off();
     const uint64_t out_body = ph[i].total - ph[i].prelearn;
     const uint64_t nchunks = (out_body + ph[i].cs - 1) / ph[i].cs;
-    status[i] = parse_batches(h[i] + body_off, ns[i] - body_off, nchunks, ph[i].batch, true, off[i], len[i]);
+    status[i] = parse_batches(h[i] + body_off, ns[i] - body_off, nchunks, ph[i].batch, true, off[i], len[i],
+                              ph[i].wide);
     if (!status[i]) ok.push_back(i);
   }
   // groups: one per unit length for model-free containers, one per prelearned container
@@ -723,9 +735,9 @@ static int decompress_containers(cucm_ctx *c, uint32_t count, const uint8_t *con
       HostModel hm;
       pre.resize(ph[i0].prelearn);
       if (ph[i0].coded)
-        hm.prelearn_decode(h[i0] + kHeaderBytes, ph[i0].pl_len, pre.data(), ph[i0].prelearn);
+        hm.prelearn_decode(h[i0] + ph[i0].hdr, ph[i0].pl_len, pre.data(), ph[i0].prelearn);
       else {
-        std::memcpy(pre.data(), h[i0] + kHeaderBytes, ph[i0].prelearn);
+        std::memcpy(pre.data(), h[i0] + ph[i0].hdr, ph[i0].prelearn);
         hm.prelearn_train(pre.data(), ph[i0].prelearn);
       }
       hm.to_device(image, ms.init);
@@ -739,7 +751,7 @@ static int decompress_containers(cucm_ctx *c, uint32_t count, const uint8_t *con
       const uint32_t i = grp[j];
       bat[j] = btot;
       oat[j] = otot;
-      btot += ((ns[i] - kHeaderBytes - ph[i].pl_len) + 15) & ~15ull;
+      btot += ((ns[i] - ph[i].body_off()) + 15) & ~15ull;
       otot += ((ph[i].total - ph[i].prelearn) + 15) & ~15ull;
     }
     if (!dev) {
@@ -749,7 +761,7 @@ static int decompress_containers(cucm_ctx *c, uint32_t count, const uint8_t *con
     std::vector<DecJob> jobs(grp.size());
     for (size_t j = 0; j < grp.size(); j++) {
       const uint32_t i = grp[j];
-      const uint64_t body_off = kHeaderBytes + ph[i].pl_len;
+      const uint64_t body_off = ph[i].body_off();
       const uint64_t body_n = ns[i] - body_off;
       DecJob &jb = jobs[j];
       if (dev) {
@@ -841,9 +853,9 @@ int cucm_model_from_container(const uint8_t *in, uint64_t n, cucm_model **out) {
     HostModel hm;
     std::vector<uint8_t> pre(ph.prelearn);
     if (ph.coded)
-      hm.prelearn_decode(in + kHeaderBytes, ph.pl_len, pre.data(), ph.prelearn);
+      hm.prelearn_decode(in + ph.hdr, ph.pl_len, pre.data(), ph.prelearn);
     else
-      hm.prelearn_train(in + kHeaderBytes, ph.prelearn);
+      hm.prelearn_train(in + ph.hdr, ph.prelearn);
     hm.to_device(m->image, m->init);
   } catch (const std::bad_alloc &) {
     return CUCM_ENOMEM;
@@ -866,8 +878,10 @@ static int compress_body(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint64_t 
   model_source(m, ms);
   Encoded e;
   int rc = encode_chunks(c, {Seg{d_in, n}}, chunksize, unit, ms, c->d_body.cap + c->d_out.cap, e);
-  const uint64_t body_n = rc ? 0 : layout_body(e, 0, 0xffff, false, nullptr, nullptr);
+  bool overflow = false;
+  const uint64_t body_n = rc ? 0 : layout_body(e, 0, 0xffff, false, nullptr, nullptr, false, &overflow);
   *out_n = body_n;
+  if (!rc && overflow) rc = CUCM_EINVAL;
   if (!rc && body_n > cap) rc = CUCM_ENOSPC;
   if (!rc && body_n) {
     uint8_t *dst = d_out;
@@ -889,6 +903,7 @@ static int batch_args(uint64_t n, uint64_t chunksize, uint32_t unit) {
   p.chunksize = chunksize;
   p.unit = unit;
   p.batch = 0xffff;
+  p.format = CUCM_FORMAT_32;  // a batch body's end offsets are 32-bit
   int rc = check_params(&p, n);
   if (rc) return rc;
   return (n + chunksize - 1) / chunksize > 0xffff ? CUCM_EINVAL : CUCM_OK;
@@ -1019,23 +1034,23 @@ int cucm_frame_bodies(const cucm_params *p, uint64_t orig_size, uint32_t nbodies
   std::unique_ptr<HostModel> hm;
   rc = make_header(nullptr, orig_size, p, hdr, hm);
   if (rc) return rc;
-  const uint64_t body = layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, nullptr, nullptr);
+  const bool wide = wide_format(p, orig_size);
+  bool overflow = false;
+  const uint64_t body =
+      layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, nullptr, nullptr, wide, &overflow);
+  if (overflow) return CUCM_EINVAL;
   *out_n = hdr.size() + body;
   if (*out_n > cap) return CUCM_ENOSPC;
   if (!out) return CUCM_EINVAL;
   std::memcpy(out, hdr.data(), hdr.size());
   std::vector<PackEntry> pe;
-  layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, out + hdr.size(), &pe);
+  layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, out + hdr.size(), &pe, wide);
+  const int fw = wide ? 8 : 4;
   for (const PackEntry &e : pe) {
     if (e.len) std::memcpy(e.base + e.dst, e.src, e.len);
-    put_be32(e.base + e.table_at, e.end_value);
-    if (e.size_at != ~0ull) {
-      uint8_t *z = e.base + e.size_at;
-      z[0] = (uint8_t)e.batch_size;
-      z[1] = (uint8_t)(e.batch_size >> 8);
-      z[2] = (uint8_t)(e.batch_size >> 16);
-      z[3] = (uint8_t)(e.batch_size >> 24);
-    }
+    for (int b = 0; b < fw; b++) e.base[e.table_at + b] = (uint8_t)(e.end_value >> (8 * (fw - 1 - b)));
+    if (e.size_at != ~0ull)
+      for (int b = 0; b < fw; b++) e.base[e.size_at + b] = (uint8_t)(e.batch_size >> (8 * b));
   }
   return CUCM_OK;
 }
@@ -1064,13 +1079,17 @@ int cucm_frame_bodies_dev(cucm_ctx *c, const cucm_params *p, uint64_t orig_size,
   std::unique_ptr<HostModel> hm;
   rc = make_header(nullptr, orig_size, p, hdr, hm);
   if (rc) return rc;
-  const uint64_t body = layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, nullptr, nullptr);
+  const bool wide = wide_format(p, orig_size);
+  bool overflow = false;
+  const uint64_t body =
+      layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, nullptr, nullptr, wide, &overflow);
+  if (overflow) return CUCM_EINVAL;
   *out_n = hdr.size() + body;
   if (*out_n > cap) return CUCM_ENOSPC;
   if (!d_out) return CUCM_EINVAL;
   CK(cudaMemcpyAsync(d_out, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, c->stream));
   std::vector<PackEntry> pe;
-  layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, d_out + hdr.size(), &pe);
+  layout_chunks(lens.data(), src.data(), lens.size(), p->batch, true, d_out + hdr.size(), &pe, wide);
   rc = pack_bodies(c, pe);
   timing_end(c);
   CK(cudaStreamSynchronize(c->stream));
@@ -1084,12 +1103,13 @@ int cucm_decompress_range_dev(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint
   CK(cudaSetDevice(c->device));
   *out_n = 0;
   if (n < kHeaderBytes) return CUCM_EFORMAT;
-  uint8_t hb[kHeaderBytes];
-  CK(cudaMemcpy(hb, d_in, kHeaderBytes, cudaMemcpyDeviceToHost));
+  uint8_t hb[kHeaderBytes64] = {0};
+  CK(cudaMemcpy(hb, d_in, std::min<uint64_t>(n, kHeaderBytes64), cudaMemcpyDeviceToHost));
   Parsed ph;
   int rc = parse_header(hb, n, ph);  // also checks that the prelearn block lies inside the n bytes
   if (rc) return rc;
-  const uint64_t body_off = kHeaderBytes + ph.pl_len;
+  const uint64_t body_off = ph.body_off();
+  const uint64_t fw = ph.wide ? 8 : 4;
   const uint64_t out_body = ph.total - ph.prelearn;
   const uint64_t nchunks = (out_body + ph.cs - 1) / ph.cs;
   if (first > nchunks || count > nchunks - first) return CUCM_EINVAL;
@@ -1102,7 +1122,7 @@ int cucm_decompress_range_dev(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint
   std::vector<uint8_t> image;
   if (ph.prelearn) {
     std::vector<uint8_t> blk(ph.pl_len), pre(ph.prelearn);
-    CK(cudaMemcpy(blk.data(), d_in + kHeaderBytes, ph.pl_len, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(blk.data(), d_in + ph.hdr, ph.pl_len, cudaMemcpyDeviceToHost));
     HostModel hm;
     if (ph.coded)
       hm.prelearn_decode(blk.data(), ph.pl_len, pre.data(), ph.prelearn);
@@ -1123,23 +1143,23 @@ int cucm_decompress_range_dev(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint
   const uint64_t body_n = n - body_off;
   for (uint64_t k0 = 0; k0 < first + count; k0 += ph.batch) {
     const uint64_t k1 = std::min<uint64_t>(k0 + ph.batch, nchunks), C = k1 - k0;
-    uint8_t sz[4];
-    if (r + 4 > body_n) return CUCM_EFORMAT;
-    CK(cudaMemcpy(sz, d_in + body_off + r, 4, cudaMemcpyDeviceToHost));
-    const uint64_t bsz = get_le32(sz);
-    r += 4;
-    if (bsz < 4 * C || r + bsz > body_n) return CUCM_EFORMAT;
+    uint8_t sz[8];
+    if (r + fw > body_n) return CUCM_EFORMAT;
+    CK(cudaMemcpy(sz, d_in + body_off + r, fw, cudaMemcpyDeviceToHost));
+    const uint64_t bsz = get_le(sz, ph.wide);
+    r += fw;
+    if (bsz < fw * C || bsz > body_n - r) return CUCM_EFORMAT;
     if (k1 > first) {
-      std::vector<uint8_t> tab(4 * C);
-      CK(cudaMemcpy(tab.data(), d_in + body_off + r, 4 * C, cudaMemcpyDeviceToHost));
+      std::vector<uint8_t> tab(fw * C);
+      CK(cudaMemcpy(tab.data(), d_in + body_off + r, fw * C, cudaMemcpyDeviceToHost));
       uint64_t start = 0;
       for (uint64_t k = k0; k < k1; k++) {
-        const uint64_t endv = get_be32(&tab[4 * (k - k0)]);
-        if (endv + 1 < 4 * C) return CUCM_EFORMAT;
-        const uint64_t end = endv + 1 - 4 * C;
-        if (end < start || end > bsz - 4 * C) return CUCM_EFORMAT;
+        const uint64_t endv = get_be(&tab[fw * (k - k0)], ph.wide);
+        if (endv + 1 < fw * C) return CUCM_EFORMAT;
+        const uint64_t end = endv + 1 - fw * C;
+        if (end < start || end > bsz - fw * C) return CUCM_EFORMAT;
         if (k >= first && k < first + count) {
-          jb.off.push_back(r + 4 * C + start);
+          jb.off.push_back(r + fw * C + start);
           jb.len.push_back(end - start);
         }
         start = end;

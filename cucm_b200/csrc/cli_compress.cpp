@@ -121,7 +121,9 @@ int main(int argc, char **argv) {
   auto t1 = std::chrono::high_resolution_clock::now();
   uint64_t nchunks = n > p.prelearn ? (n - p.prelearn + p.chunksize - 1) / p.chunksize : 0;
   uint64_t nbatches = (nchunks + p.batch - 1) / p.batch;
-  uint64_t reported = out_n - 4 * nbatches;  // the reference's count leaves out the batch size fields
+  // the reference's count leaves out the batch size fields (8 bytes each in
+  // the 64-bit container, which inputs past 4 GiB get)
+  uint64_t reported = out_n - (n > 0xffffffffull ? 8 : 4) * nbatches;
   std::cout << "Original size  : " << n << " bytes\n";
   std::cout << "Compressed size: " << reported << " bytes\n";
   std::cout << "Compression ratio: " << (reported ? (double)n / (double)reported : 0.0) << "\n";

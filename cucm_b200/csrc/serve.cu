@@ -168,19 +168,19 @@ int prepare(Req *r) {
   if (r->ph.total > r->cap || (!r->out && r->ph.total)) return CUCM_ENOSPC;
   r->unit = r->ph.unit;
   r->cs = r->ph.cs;
-  r->body_off = kHeaderBytes + r->ph.pl_len;
+  r->body_off = r->ph.body_off();
   r->body_n = r->n - r->body_off;
   r->out_body = r->ph.total - r->ph.prelearn;
   r->nchunks = (r->out_body + r->cs - 1) / r->cs;
-  rc = parse_batches(r->in + r->body_off, r->body_n, r->nchunks, r->ph.batch, true, r->off, r->len);
+  rc = parse_batches(r->in + r->body_off, r->body_n, r->nchunks, r->ph.batch, true, r->off, r->len, r->ph.wide);
   if (rc) return rc;
   if (r->ph.prelearn) {
     r->hm.reset(new HostModel());
     r->pre.resize(r->ph.prelearn);
     if (r->ph.coded)
-      r->hm->prelearn_decode(r->in + kHeaderBytes, r->ph.pl_len, r->pre.data(), r->ph.prelearn);
+      r->hm->prelearn_decode(r->in + r->ph.hdr, r->ph.pl_len, r->pre.data(), r->ph.prelearn);
     else {
-      std::memcpy(r->pre.data(), r->in + kHeaderBytes, r->ph.prelearn);
+      std::memcpy(r->pre.data(), r->in + r->ph.hdr, r->ph.prelearn);
       r->hm->prelearn_train(r->pre.data(), r->ph.prelearn);
     }
   }
@@ -503,10 +503,12 @@ int after_encode(cucm_server *s, Launch *l) {
   uint64_t tot = 0;
   for (size_t j = 0; j < l->reqs.size(); j++) {
     Req *r = l->reqs[j];
+    bool overflow = false;
     body[j] = layout_chunks(l->h_lens + l->first[j], src.data() + l->first[j], r->nchunks, r->p.batch, true, nullptr,
-                            nullptr);
+                            nullptr, wide_format(&r->p, r->n), &overflow);
     r->out_n = r->hdr.size() + body[j];
-    if (r->out_n > r->cap) r->status = CUCM_ENOSPC;
+    if (overflow) r->status = CUCM_EINVAL;  // a batch past 4 GiB needs the 64-bit container
+    else if (r->out_n > r->cap) r->status = CUCM_ENOSPC;
     at[j] = tot;
     tot += (body[j] + 15) & ~15ull;
   }
@@ -518,7 +520,7 @@ int after_encode(cucm_server *s, Launch *l) {
     Req *r = l->reqs[j];
     if (r->status) continue;
     layout_chunks(l->h_lens + l->first[j], src.data() + l->first[j], r->nchunks, r->p.batch, true, d_out + at[j],
-                  &pe);
+                  &pe, wide_format(&r->p, r->n));
   }
   if (!pe.empty()) {
     PackEntry *d_pe = (PackEntry *)dalloc(l, sizeof(PackEntry) * pe.size(), &err);

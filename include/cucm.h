@@ -51,7 +51,18 @@ typedef struct cucm_params {
   uint32_t unit;      /* -u, bits per unit (default 128); multiple of 32, <= 1024 */
   uint64_t prelearn;  /* -p, bytes of host prelearn prefix (default 0) */
   uint32_t batch;     /* -b, chunks per container batch (default 100); stored as u16 */
+  uint32_t format;    /* container: CUCM_FORMAT_AUTO (default), _32 or _64 */
 } cucm_params;
+
+/* Container formats.  _32 is the reference's (cucm_compress_v2.cu:1197-1244):
+ * its size fields are 32 bits, so it holds at most 4 GiB of input.  _64 has
+ * no counterpart in the reference: the same chunk payloads behind a 45-byte
+ * header with 64-bit sizes (first bytes ff ff ff ff 00 00 00 02, which a
+ * 32-bit reader refuses) and 64-bit batch sizes and end offsets.  _AUTO
+ * writes _32 up to 4 GiB of input and _64 beyond.  Decompression reads both. */
+#define CUCM_FORMAT_AUTO 0u
+#define CUCM_FORMAT_32 1u
+#define CUCM_FORMAT_64 2u
 
 /* Execution choices.  None of them changes a single output byte. */
 typedef enum cucm_form {
@@ -89,7 +100,7 @@ int cucm_ctx_get_tuning(cucm_ctx *ctx, cucm_tuning *tuning);
 /* Largest container cucm_compress can produce for n input bytes. */
 uint64_t cucm_compress_bound(uint64_t n, const cucm_params *p);
 /* Original size recorded in a container header (first 4 bytes, big endian,
- * cucm_decompress_v2.cu:1298-1301). */
+ * cucm_decompress_v2.cu:1298-1301; bytes 8..15 of the 64-bit container). */
 int cucm_decompressed_size(const uint8_t *in, uint64_t n, uint64_t *size);
 
 /* Whole container: the output of `cucm_compress -f IN -s -u -p -b`
