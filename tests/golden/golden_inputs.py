@@ -66,4 +66,12 @@ CASES = [
     _c("text_0_cs4k", "text", 0, 8, 4096),
     _c("text_4097_cs4096_u64", "text", 4097, 9, 4096, unit=64, batch=1),
     _c("text_8192_cs4096", "text", 8192, 10, 4096),
+    # edge sizes around one unit (16 bytes at unit 128) and one chunk
+    _c("text_8_cs4k", "text", 8, 11, 4096),
+    _c("text_15_cs4k", "text", 15, 11, 4096),
+    _c("text_16_cs4k", "text", 16, 11, 4096),
+    _c("text_17_cs4k", "text", 17, 11, 4096),
+    _c("walk_4095_cs4096", "walk", 4095, 12, 4096),
+    _c("walk_4097_cs4096", "walk", 4097, 12, 4096),
+    _c("text_40k_pre16k", "text", 40000, 13, 4096, prelearn=16384),
 ]
