@@ -18,7 +18,8 @@ import functools
 import os
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libcucm.so")
+# the in-tree build; CUCM_LIBRARY names another build of the same library
+LIB_PATH = os.environ.get("CUCM_LIBRARY") or os.path.join(_PKG, "libcucm.so")
 
 FORM_AUTO, FORM_PLAIN, FORM_PERSISTENT = 0, 1, 2
 
