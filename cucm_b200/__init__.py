@@ -45,7 +45,8 @@ FORMAT_AUTO, FORMAT_32, FORMAT_64 = 0, 1, 2
 
 class Params(ctypes.Structure):
     _fields_ = [("chunksize", ctypes.c_uint64), ("unit", ctypes.c_uint32),
-                ("prelearn", ctypes.c_uint64), ("batch", ctypes.c_uint32), ("format", ctypes.c_uint32)]
+                ("prelearn", ctypes.c_uint64), ("batch", ctypes.c_uint32), ("format", ctypes.c_uint32),
+                ("fixed_model", ctypes.c_uint32)]
 
 
 class Stats(ctypes.Structure):
@@ -174,11 +175,14 @@ def lib():
     return L
 
 
-def default_params(chunksize=None, unit=None, prelearn=None, batch=None, fmt=None):
+def default_params(chunksize=None, unit=None, prelearn=None, batch=None, fmt=None, fixed=None):
     """cucm_params: the reference CLI's defaults, then the given fields; fmt
-    is the container format (FORMAT_AUTO, FORMAT_32 or FORMAT_64)."""
+    is the container format (FORMAT_AUTO, FORMAT_32 or FORMAT_64), fixed the
+    fixed-model variant (needs a prelearn prefix)."""
     p = Params()
     lib().cucm_default_params(ctypes.byref(p))
+    if fixed is not None:
+        p.fixed_model = 1 if fixed else 0
     if fmt is not None:
         p.format = int(fmt)
     if chunksize is not None:
@@ -319,11 +323,13 @@ class Context:
                  for r in res[:min(count.value, 64)]]
         return _tuning_dict(best), cands
 
-    def compress(self, data, chunksize=1 << 20, unit=128, prelearn=0, batch=100, fmt=FORMAT_AUTO, out=None):
+    def compress(self, data, chunksize=1 << 20, unit=128, prelearn=0, batch=100, fmt=FORMAT_AUTO, out=None,
+                 fixed=False):
         """The container of `data`.  With `out` (a writable numpy uint8 array)
         the container is written there and a view of it returned; otherwise
-        bytes, in a buffer of the compress bound."""
-        p = default_params(chunksize, unit, prelearn, batch, fmt)
+        bytes, in a buffer of the compress bound.  `fixed`: the fixed-model
+        variant (prelearn > 0)."""
+        p = default_params(chunksize, unit, prelearn, batch, fmt, fixed)
         ptr, n, keep = _buf(data)
         got = ctypes.c_uint64()
         if out is not None:

@@ -51,7 +51,7 @@ struct cucm_ctx {
   uint32_t nslots = 0;
   DevBuf image;    // prelearned slot image (when used)
   DevBuf d_init;   // ModelInit
-  DevBuf d_tasks, d_results, d_queue, d_status, d_scratch, d_big, d_pack, d_body, d_out, d_tails;
+  DevBuf d_tasks, d_results, d_queue, d_status, d_scratch, d_big, d_pack, d_body, d_out, d_tails, d_prm, d_first;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around the engine launches
   double last_ms = 0.0;
@@ -397,6 +397,140 @@ struct DecJob {
 };
 
 // Decode every chunk of every job in one engine run.
+// The fixed-model variant (fixed_model.cuh): the model is only read, so the
+// coder inputs of every chunk are computed at once (in slices of at most
+// kFixedSlice input bytes: 16 bytes of inputs per input byte), then one coder
+// thread per chunk codes them.  Same scratch and overflow handling as
+// encode_chunks.
+constexpr uint64_t kFixedSlice = 256ull << 20;
+
+int run_fixed_encode(cucm_ctx *c, std::vector<FixedTask> &tasks, const std::vector<uint64_t> &lens) {
+  // slices of consecutive tasks
+  size_t k0 = 0;
+  while (k0 < tasks.size()) {
+    uint64_t tot = 0;
+    size_t k1 = k0;
+    std::vector<uint64_t> first;
+    while (k1 < tasks.size() && (k1 == k0 || tot + lens[k1] <= kFixedSlice)) {
+      first.push_back(tot);
+      tot += lens[k1];
+      k1++;
+    }
+    CK(c->d_prm.ensure(16 * std::max<uint64_t>(tot, 1)));
+    for (size_t k = k0; k < k1; k++) tasks[k].prm = c->d_prm.as<uint16_t>() + 8 * first[k - k0];
+    const uint32_t n = (uint32_t)(k1 - k0);
+    CK(c->d_tasks.ensure(sizeof(FixedTask) * n));
+    CK(c->d_first.ensure(sizeof(uint64_t) * n));
+    CK(cudaMemcpyAsync(c->d_tasks.p, tasks.data() + k0, sizeof(FixedTask) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_first.p, first.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(launch_fixed_encode(c->d_tasks.as<FixedTask>(), c->d_first.as<uint64_t>(), n, tot, c->image.as<uint8_t>(),
+                           c->d_init.as<ModelInit>(), c->d_status.as<uint32_t>(), c->sm_count, c->stream));
+    c->launches += 2;
+    // the tasks and offsets are read by the kernels before the next slice overwrites them
+    CK(cudaStreamSynchronize(c->stream));
+    k0 = k1;
+  }
+  return CUCM_OK;
+}
+
+int encode_fixed(cucm_ctx *c, const std::vector<Seg> &segs, uint64_t cs, const ModelSource &ms, Encoded &e) {
+  e.first.assign(1, 0);
+  for (const Seg &g : segs) e.first.push_back(e.first.back() + (g.n + cs - 1) / cs);
+  const uint64_t nchunks = e.first.back();
+  e.lens.assign(nchunks, 0);
+  e.src.assign(nchunks, nullptr);
+  if (nchunks == 0) return CUCM_OK;
+  int rc = upload_model(c, ms);
+  if (rc) return rc;
+  CK(c->d_status.ensure(sizeof(uint32_t)));
+  CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(uint32_t), c->stream));
+  const uint64_t scap = scratch_cap(cs);
+  CK(c->d_scratch.ensure(scap * nchunks));
+  CK(c->d_results.ensure(sizeof(uint64_t) * nchunks));
+  std::vector<FixedTask> tasks(nchunks);
+  std::vector<uint64_t> lens(nchunks);
+  for (size_t g = 0; g < segs.size(); g++) {
+    for (uint64_t k = e.first[g]; k < e.first[g + 1]; k++) {
+      const uint64_t j = k - e.first[g];
+      FixedTask &t = tasks[k];
+      t.in = segs[g].d_in + j * cs;
+      t.in_len = lens[k] = std::min<uint64_t>(cs, segs[g].n - j * cs);
+      t.out = c->d_scratch.as<uint8_t>() + k * scap;
+      t.out_cap = scap;
+      t.prm = nullptr;
+      t.result = c->d_results.as<uint64_t>() + k;
+      e.src[k] = t.out;
+    }
+  }
+  collect_kernel_ms(c);
+  c->chunks += nchunks;
+  CK(cudaEventRecord(c->evk0, c->stream));
+  rc = run_fixed_encode(c, tasks, lens);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(e.lens.data(), c->d_results.p, sizeof(uint64_t) * nchunks, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<FixedTask> redo;
+  std::vector<uint64_t> redo_lens, redo_k;
+  for (uint64_t k = 0; k < nchunks; k++)
+    if (e.lens[k] > scap) redo_k.push_back(k);
+  if (!redo_k.empty()) {
+    const uint64_t hc = hard_cap(cs);
+    CK(c->d_big.ensure(hc * redo_k.size()));
+    for (size_t i = 0; i < redo_k.size(); i++) {
+      FixedTask t = tasks[redo_k[i]];
+      t.out = c->d_big.as<uint8_t>() + i * hc;
+      t.out_cap = hc;
+      e.src[redo_k[i]] = t.out;
+      redo.push_back(t);
+      redo_lens.push_back(lens[redo_k[i]]);
+    }
+    rc = run_fixed_encode(c, redo, redo_lens);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(e.lens.data(), c->d_results.p, sizeof(uint64_t) * nchunks, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (uint64_t k : redo_k)
+      if (e.lens[k] > hc) return CUCM_ECUDA;
+  }
+  CK(cudaEventRecord(c->evk1, c->stream));
+  c->kernel_pending = true;
+  return CUCM_OK;
+}
+
+// Decode every chunk of fixed-model containers: one warp per chunk.
+int decode_fixed(cucm_ctx *c, const std::vector<DecJob> &jobs, const ModelSource &ms) {
+  std::vector<FixedTask> tasks;
+  for (const DecJob &j : jobs)
+    for (uint64_t k = 0; k < j.off.size(); k++) {
+      FixedTask t;
+      t.in = j.d_body + j.off[k];
+      t.in_len = j.len[k];
+      t.out = j.d_out + k * j.cs;
+      t.out_cap = std::min<uint64_t>(j.cs, j.total - k * j.cs);
+      t.prm = nullptr;
+      t.result = nullptr;
+      tasks.push_back(t);
+    }
+  if (tasks.empty()) return CUCM_OK;
+  int rc = upload_model(c, ms);
+  if (rc) return rc;
+  collect_kernel_ms(c);
+  c->chunks += tasks.size();
+  CK(c->d_tasks.ensure(sizeof(FixedTask) * tasks.size()));
+  CK(cudaMemcpyAsync(c->d_tasks.p, tasks.data(), sizeof(FixedTask) * tasks.size(), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(c->d_queue.ensure(2 * sizeof(uint32_t)));
+  CK(cudaMemsetAsync(c->d_queue.p, 0, 2 * sizeof(uint32_t), c->stream));
+  CK(cudaEventRecord(c->evk0, c->stream));
+  CK(launch_fixed_decode(c->d_tasks.as<FixedTask>(), (uint32_t)tasks.size(), c->image.as<uint8_t>(),
+                         c->d_init.as<ModelInit>(), c->d_queue.as<uint32_t>(), c->sm_count, c->stream));
+  CK(cudaEventRecord(c->evk1, c->stream));
+  c->kernel_pending = true;
+  c->launches += 1;
+  CK(cudaStreamSynchronize(c->stream));
+  return CUCM_OK;
+}
+
 int decode_jobs(cucm_ctx *c, const std::vector<DecJob> &jobs, uint32_t unit, const ModelSource &ms,
                 uint64_t other_bytes) {
   std::vector<ChunkTask> tasks;
@@ -438,6 +572,7 @@ void cucm_default_params(cucm_params *p) {
   p->prelearn = 0;
   p->batch = 100;              // cucm_compress_v2.cu:1312
   p->format = CUCM_FORMAT_AUTO;
+  p->fixed_model = 0;
 }
 
 const char *cucm_strerror(int s) {
@@ -607,7 +742,8 @@ static int compress_containers(cucm_ctx *c, uint32_t count, const uint8_t *const
       }
     }
     Encoded e;
-    rc = encode_chunks(c, segs, p->chunksize, p->unit, ms, c->d_body.cap + c->d_out.cap, e);
+    rc = p->fixed_model ? encode_fixed(c, segs, p->chunksize, ms, e)
+                        : encode_chunks(c, segs, p->chunksize, p->unit, ms, c->d_body.cap + c->d_out.cap, e);
     if (rc) break;
     std::vector<uint64_t> body(grp.size()), at(grp.size());
     uint64_t stage = 0;
@@ -780,7 +916,7 @@ static int decompress_containers(cucm_ctx *c, uint32_t count, const uint8_t *con
       jb.total = ph[i].total - ph[i].prelearn;
       jb.cs = ph[i].cs;
     }
-    rc = decode_jobs(c, jobs, ph[i0].unit, ms, c->d_body.cap + c->d_out.cap);
+    rc = ph[i0].fixed ? decode_fixed(c, jobs, ms) : decode_jobs(c, jobs, ph[i0].unit, ms, c->d_body.cap + c->d_out.cap);
     if (rc) {
       for (uint32_t i : grp) status[i] = rc;
       if (rc == CUCM_EFORMAT) {
@@ -1108,6 +1244,7 @@ int cucm_decompress_range_dev(cucm_ctx *c, const uint8_t *d_in, uint64_t n, uint
   Parsed ph;
   int rc = parse_header(hb, n, ph);  // also checks that the prelearn block lies inside the n bytes
   if (rc) return rc;
+  if (ph.fixed) return CUCM_EINVAL;  // the adaptive streams only
   const uint64_t body_off = ph.body_off();
   const uint64_t fw = ph.wide ? 8 : 4;
   const uint64_t out_body = ph.total - ph.prelearn;

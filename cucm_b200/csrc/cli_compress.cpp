@@ -21,6 +21,8 @@ static void print_help(const char *prog) {
             << "  -o, --output <path>   Output compressed file (default: ./compressed.bin)\n"
             << "  -p, --prelearn <SZ>   Prelearn size, supports K/M/G suffix (default: 0 = disabled)\n"
             << "  -b, --batch <NUM>     Chunks per container batch (default: 100)\n"
+            << "  -F, --fixed           Fixed-model variant: code with the prelearned model, no updates\n"
+            << "                        (needs -p; not a reference stream)\n"
             << "  -d, --device <ID>     CUDA device (default: 0)\n"
             << "  -h, --help            Show this help message\n";
 }
@@ -70,6 +72,8 @@ int main(int argc, char **argv) {
         std::cerr << "Invalid batch number: " << batch << std::endl;
         return 1;
       }
+    } else if (std::strcmp(argv[i], "-F") == 0 || std::strcmp(argv[i], "--fixed") == 0) {
+      p.fixed_model = 1;
     } else if (is("-d", "--device")) {
       device = std::atoi(argv[++i]);
     } else if (std::strcmp(argv[i], "-h") == 0 || std::strcmp(argv[i], "--help") == 0) {
@@ -83,6 +87,10 @@ int main(int argc, char **argv) {
   }
   p.unit = (uint32_t)unit;
   p.batch = (uint32_t)batch;
+  if (p.fixed_model && p.prelearn == 0) {
+    std::cerr << "The fixed-model variant (-F) needs a prelearn prefix (-p)" << std::endl;
+    return 1;
+  }
   std::vector<uint8_t> data;
   if (!cucm_cli::read_file(in_path.c_str(), data)) {
     std::cerr << "Failed to open input file: " << in_path << std::endl;

@@ -139,6 +139,7 @@ inline int check_params(const cucm_params *p, uint64_t n) {
   if (p->batch == 0 || p->batch > 0xffff) return CUCM_EINVAL;
   if (p->prelearn > n) return CUCM_EINVAL;
   if (p->format != CUCM_FORMAT_AUTO && p->format != CUCM_FORMAT_32 && p->format != CUCM_FORMAT_64) return CUCM_EINVAL;
+  if (p->fixed_model > 1 || (p->fixed_model && p->prelearn == 0)) return CUCM_EINVAL;  // the variant needs a prelearned model
   if (!wide_format(p, n) && n > 0xffffffffull) return CUCM_EINVAL;  // the 32-bit header holds the size
   return CUCM_OK;
 }
@@ -166,7 +167,7 @@ inline int make_header(const uint8_t *in, uint64_t n, const cucm_params *p, std:
     put_be32(&hdr[8], (uint32_t)p->chunksize);
     put_be32(&hdr[12], (uint32_t)coded);
     put_be32(&hdr[16], (uint32_t)p->prelearn);
-    hdr[20] = raw ? 0 : 1;
+    hdr[20] = (uint8_t)((raw ? 0 : 1) | (p->fixed_model ? 2 : 0));
   } else {
     put_be32(&hdr[0], 0xffffffffu);  // bytes 4..5 stay zero
     hdr[7] = 2;
@@ -176,7 +177,7 @@ inline int make_header(const uint8_t *in, uint64_t n, const cucm_params *p, std:
     put_be32(&hdr[24], (uint32_t)p->chunksize);
     put_be64(&hdr[28], coded);
     put_be64(&hdr[36], p->prelearn);
-    hdr[44] = raw ? 0 : 1;
+    hdr[44] = (uint8_t)((raw ? 0 : 1) | (p->fixed_model ? 2 : 0));
   }
   if (pl_len) std::memcpy(&hdr[hl], raw ? in : pl.data(), pl_len);
   return CUCM_OK;
@@ -186,6 +187,8 @@ struct Parsed {
   uint64_t total, cs, prelearn, pl_coded, pl_len;
   uint32_t batch, unit;
   int coded;
+  int flag;      // flag byte: bit 0 coded prelearn block, bit 1 fixed model
+  bool fixed;    // the fixed-model variant
   bool wide;     // the 64-bit container
   uint64_t hdr;  // header bytes (21 or 45); the prelearn block follows
   uint64_t body_off() const { return hdr + pl_len; }
@@ -207,7 +210,7 @@ inline int parse_header(const uint8_t *in, uint64_t n, Parsed &h) {
     h.cs = get_be32(in + 8);
     h.pl_coded = get_be32(in + 12);
     h.prelearn = get_be32(in + 16);
-    h.coded = in[20];
+    h.flag = in[20];
   } else {
     if (n < kHeaderBytes64) return CUCM_EFORMAT;
     h.hdr = kHeaderBytes64;
@@ -217,10 +220,15 @@ inline int parse_header(const uint8_t *in, uint64_t n, Parsed &h) {
     h.cs = get_be32(in + 24);
     h.pl_coded = get_be64(in + 28);
     h.prelearn = get_be64(in + 36);
-    h.coded = in[44];
+    h.flag = in[44];
   }
   if (h.cs == 0 || h.batch == 0 || h.unit < 32 || h.unit > (uint32_t)kMaxUnit || h.unit % 32) return CUCM_EFORMAT;
   if (h.prelearn > h.total) return CUCM_EFORMAT;
+  // flag bit 0: the prelearn block is coded; bit 1: the fixed-model variant
+  // (which needs the prelearned model)
+  if (h.flag > 3 || ((h.flag & 2) && h.prelearn == 0)) return CUCM_EFORMAT;
+  h.coded = h.flag & 1;
+  h.fixed = (h.flag & 2) != 0;
   h.pl_len = h.coded ? h.pl_coded : h.prelearn;
   if (h.pl_len > n || h.hdr + h.pl_len > n) return CUCM_EFORMAT;
   return CUCM_OK;

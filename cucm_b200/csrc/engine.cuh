@@ -44,6 +44,19 @@ struct TailTask {
   uint16_t prm[256];  // the last data unit's buffer (units up to 256 bits)
 };
 
+// One chunk of a fixed-model launch (the variant without online updates).
+// compress: in = the chunk's bytes, prm = room for its coder inputs (8 u16
+// per byte, 16-byte aligned), out = payload scratch; decompress: in = the
+// payload, out = the chunk's bytes.
+struct FixedTask {
+  const uint8_t *in;
+  uint64_t in_len;   // compress: chunk bytes; decompress: payload bytes
+  uint8_t *out;
+  uint64_t out_cap;  // compress: payload capacity; decompress: chunk bytes
+  uint16_t *prm;
+  uint64_t *result;  // compress: payload length
+};
+
 // Status words written by the kernels (per launch).
 enum DevStatus : uint32_t {
   kDevOk = 0,
@@ -78,6 +91,16 @@ cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *
 cudaError_t launch_decompress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *slots, uint32_t nslots,
                               const uint8_t *init_tables, const ModelInit *d_init, uint32_t *d_queue,
                               uint32_t *d_status, const EngineConfig &cfg, cudaStream_t stream, int unit);
+
+// Fixed-model variant: coder inputs of every byte of every task (first[]:
+// prefix sums of the chunk lengths, total bytes), then one coder thread per
+// task; and the decoder, one warp per task from a zeroed queue counter.
+// image / d_init: the prelearned model in the device layout.
+cudaError_t launch_fixed_encode(const FixedTask *d_tasks, const uint64_t *d_first, uint32_t ntasks, uint64_t total,
+                                const uint8_t *image, const ModelInit *d_init, uint32_t *d_status, int sm_count,
+                                cudaStream_t stream);
+cudaError_t launch_fixed_decode(const FixedTask *d_tasks, uint32_t ntasks, const uint8_t *image,
+                                const ModelInit *d_init, uint32_t *d_queue, int sm_count, cudaStream_t stream);
 
 size_t compress_smem_bytes(int unit);
 // Chunk slots of the engine that run at once on one SM.

@@ -539,6 +539,7 @@ __global__ void __launch_bounds__(256) decompress_kernel(const ChunkTask *tasks,
 
 #include "compress_fast.cuh"
 #include "decompress_fast.cuh"
+#include "fixed_model.cuh"
 
 }  // namespace
 
@@ -549,6 +550,32 @@ int compress_threads(int unit) { return unit <= kFastMaxUnit ? kFastThreads : 25
 size_t decompress_smem_bytes(int unit, int spec_bits) {
   (void)spec_bits;
   return make_layout(unit, 0).total + kNodeBytes;
+}
+
+cudaError_t launch_fixed_encode(const FixedTask *d_tasks, const uint64_t *d_first, uint32_t ntasks, uint64_t total,
+                                const uint8_t *image, const ModelInit *d_init, uint32_t *d_status, int sm_count,
+                                cudaStream_t stream) {
+  if (ntasks == 0) return cudaSuccess;
+  if (total) {
+    const uint64_t blocks = (total + kFixedThreads - 1) / kFixedThreads;
+    const uint64_t cap = (uint64_t)(sm_count > 0 ? sm_count : 148) * 8;
+    fixed_prob_kernel<<<(unsigned)std::min<uint64_t>(blocks, cap), kFixedThreads, 0, stream>>>(
+        d_tasks, d_first, ntasks, total, image, d_init);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  fixed_coder_kernel<<<(ntasks + 127) / 128, 128, 0, stream>>>(d_tasks, ntasks, d_status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fixed_decode(const FixedTask *d_tasks, uint32_t ntasks, const uint8_t *image,
+                                const ModelInit *d_init, uint32_t *d_queue, int sm_count, cudaStream_t stream) {
+  if (ntasks == 0) return cudaSuccess;
+  const uint32_t want = (ntasks + kFixedDecWarps - 1) / kFixedDecWarps;
+  const uint32_t cap = (uint32_t)(sm_count > 0 ? sm_count : 148) * 4;
+  fixed_decode_kernel<<<std::min(want, cap), kFixedDecWarps * 32, 0, stream>>>(d_tasks, ntasks, image, d_init,
+                                                                              d_queue);
+  return cudaGetLastError();
 }
 
 cudaError_t upload_tables() {

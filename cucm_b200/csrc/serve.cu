@@ -153,6 +153,7 @@ int prepare(Req *r) {
   if (r->op == CUCM_OP_COMPRESS) {
     int rc = check_params(&r->p, r->n);
     if (rc) return rc;
+    if (r->p.fixed_model) return CUCM_EINVAL;  // the serving loop codes the adaptive streams
     rc = make_header(r->in, r->n, &r->p, r->hdr, r->hm);
     if (rc) return rc;
     r->unit = r->p.unit;
@@ -164,6 +165,7 @@ int prepare(Req *r) {
   }
   int rc = parse_header(r->in, r->n, r->ph);
   if (rc) return rc;
+  if (r->ph.fixed) return CUCM_EINVAL;
   r->out_n = r->ph.total;
   if (r->ph.total > r->cap || (!r->out && r->ph.total)) return CUCM_ENOSPC;
   r->unit = r->ph.unit;

@@ -52,7 +52,17 @@ typedef struct cucm_params {
   uint64_t prelearn;  /* -p, bytes of host prelearn prefix (default 0) */
   uint32_t batch;     /* -b, chunks per container batch (default 100); stored as u16 */
   uint32_t format;    /* container: CUCM_FORMAT_AUTO (default), _32 or _64 */
+  uint32_t fixed_model; /* 1: the fixed-model variant (see below); needs prelearn > 0; default 0 */
 } cucm_params;
+
+/* The fixed-model variant.  The paper behind the reference (its section 4.5)
+ * measures CuCM with the model kept fixed after the prelearn pass -- no
+ * StateMap or Mixer updates while the data is coded -- but the reference
+ * ships no code for it.  Here it is a stream of its own (container flag bit
+ * 1): every chunk is coded with the prelearned model, unchanged, over its
+ * data bits only (no stale tail).  It is not the reference's stream; its
+ * decoder is this library's.  The serving loop and the multi-GPU calls take
+ * only the reference's adaptive streams. */
 
 /* Container formats.  _32 is the reference's (cucm_compress_v2.cu:1197-1244):
  * its size fields are 32 bits, so it holds at most 4 GiB of input.  _64 has

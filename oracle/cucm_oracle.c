@@ -456,6 +456,61 @@ void co_decode_chunk(co_model *work, const uint8_t *payload, size_t plen, size_t
   unit_buf_free(&ub);
 }
 
+/* ---- fixed-model chunk coder (PDF section 4.5) --------------------------- */
+
+/* The fixed-model variant the paper discusses (section 4.5: the model is
+ * kept fixed after the prelearn pass, no online updates): every data bit of
+ * the chunk is predicted by the prelearned model exactly as the prelearn
+ * pass predicts it (prelearn_bit, i.e. cucm_compress_v2.cu:930-955 --
+ * hashes over the chunk's own history, StateMaps, Mixer) and nothing is
+ * updated.  The reference ships no code for it; this restatement defines the
+ * variant's stream.  Only the chunk's data bits are coded (no stale tail),
+ * then the flush byte. */
+size_t co_encode_chunk_fixed(const co_model *m, const uint8_t *chunk, size_t len, uint8_t *out, size_t cap) {
+  tables_once();
+  uint32_t x1 = 0, x2 = 0xffffffffu;
+  size_t off = 0;
+  uint32_t hs[CO_ORDERS];
+  int smp[CO_ORDERS], pr, cxt;
+  for (size_t pos = 0; pos < len * 8; pos++) {
+    int y = (chunk[pos >> 3] >> (7 - (pos & 7))) & 1;
+    prelearn_bit((co_model *)m, chunk, pos, y, &pr, hs, smp, &cxt);
+    uint32_t xmid = coder_mid(x1, x2, pr);
+    if (y) x2 = xmid; else x1 = xmid + 1;
+    while (((x1 ^ x2) & 0xff000000u) == 0) {
+      if (off >= cap) return (size_t)-1;
+      out[off++] = (uint8_t)(x2 >> 24);
+      x1 <<= 8;
+      x2 = (x2 << 8) | 255u;
+    }
+  }
+  if (off >= cap) return (size_t)-1;
+  out[off++] = (uint8_t)(x1 >> 24);
+  return off;
+}
+
+void co_decode_chunk_fixed(const co_model *m, const uint8_t *payload, size_t plen, size_t len, uint8_t *out) {
+  tables_once();
+  memset(out, 0, len);
+  uint32_t x1 = 0, x2 = 0xffffffffu, x = 0;
+  size_t ioff = 0;
+  for (int i = 0; i < 4; i++) x = (x << 8) | (ioff < plen ? payload[ioff++] : 255u);
+  uint32_t hs[CO_ORDERS];
+  int smp[CO_ORDERS], pr, cxt;
+  for (size_t pos = 0; pos < len * 8; pos++) {
+    prelearn_bit((co_model *)m, out, pos, 0, &pr, hs, smp, &cxt);
+    uint32_t xmid = coder_mid(x1, x2, pr);
+    int y = x <= xmid;
+    if (y) x2 = xmid; else x1 = xmid + 1;
+    while (((x1 ^ x2) & 0xff000000u) == 0) {
+      x1 <<= 8;
+      x2 = (x2 << 8) | 255u;
+      x = (x << 8) | (ioff < plen ? payload[ioff++] : 255u);
+    }
+    out[pos >> 3] |= (uint8_t)(y << (7 - (pos & 7)));
+  }
+}
+
 /* ---- container ---------------------------------------------------------- */
 
 static inline void put_be32(uint8_t *p, uint32_t v) {
@@ -495,12 +550,13 @@ typedef struct job {
   pthread_mutex_t lock;
   int err;
   int decode;
+  int fixed;            /* fixed-model variant: the shared model is only read */
 } job;
 
 static void *job_worker(void *arg) {
   job *J = (job *)arg;
-  co_model *work = co_model_new();
-  if (!work) {
+  co_model *work = J->fixed ? NULL : co_model_new();
+  if (!work && !J->fixed) {
     pthread_mutex_lock(&J->lock);
     J->err = -1;
     pthread_mutex_unlock(&J->lock);
@@ -511,13 +567,15 @@ static void *job_worker(void *arg) {
     size_t k = J->next++;
     pthread_mutex_unlock(&J->lock);
     if (k >= J->nchunks) break;
-    co_model_copy(work, J->init);
+    if (!J->fixed) co_model_copy(work, J->init);
     size_t off = k * J->cs;
     size_t len = J->n - off < J->cs ? J->n - off : J->cs;
     if (!J->decode) {
       size_t cap = co_chunk_bound(J->cs);
       uint8_t *buf = (uint8_t *)malloc(cap);
-      size_t got = buf ? co_encode_chunk(work, J->data + off, len, J->cs, J->unit, buf, cap) : (size_t)-1;
+      size_t got = !buf ? (size_t)-1
+                   : J->fixed ? co_encode_chunk_fixed(J->init, J->data + off, len, buf, cap)
+                              : co_encode_chunk(work, J->data + off, len, J->cs, J->unit, buf, cap);
       if (got == (size_t)-1) {
         free(buf);
         pthread_mutex_lock(&J->lock);
@@ -527,11 +585,13 @@ static void *job_worker(void *arg) {
       }
       J->pay[k] = buf;
       J->pay_n[k] = got;
+    } else if (J->fixed) {
+      co_decode_chunk_fixed(J->init, J->cin[k], J->cin_n[k], len, J->dout + off);
     } else {
       co_decode_chunk(work, J->cin[k], J->cin_n[k], len, J->cs, J->unit, J->dout + off);
     }
   }
-  co_model_free(work);
+  if (work) co_model_free(work);
   return NULL;
 }
 
@@ -550,11 +610,13 @@ static int run_jobs(job *J, int threads) {
   return J->err;
 }
 
-/* compress_file (cucm_compress_v2.cu:1151-1250). */
-int co_compress(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelearn, int batch, int threads,
-                uint8_t **out, size_t *out_n) {
+/* compress_file (cucm_compress_v2.cu:1151-1250); `fixed` selects the
+ * fixed-model variant (flag byte bit 1, prelearn required). */
+int co_compress_ex(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelearn, int batch, int fixed,
+                   int threads, uint8_t **out, size_t *out_n) {
   tables_once();
   if (cs == 0 || unit <= 0 || batch <= 0 || prelearn > n) return -2;
+  if (fixed && prelearn == 0) return -2;
   co_model *init = co_model_new();
   if (!init) return -1;
   size_t pl_cap = prelearn * 8 + 8;
@@ -574,6 +636,7 @@ int co_compress(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelear
   J.cs = cs;
   J.unit = unit;
   J.nchunks = nchunks;
+  J.fixed = fixed;
   J.pay = (uint8_t **)calloc(nchunks ? nchunks : 1, sizeof(uint8_t *));
   J.pay_n = (size_t *)calloc(nchunks ? nchunks : 1, sizeof(size_t));
   int rc = nchunks ? run_jobs(&J, threads) : 0;
@@ -598,7 +661,7 @@ int co_compress(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelear
   put_be32(o + 8, (uint32_t)cs);
   put_be32(o + 12, (uint32_t)pl_coded);
   put_be32(o + 16, (uint32_t)prelearn);
-  o[20] = raw ? 0 : 1;
+  o[20] = (uint8_t)((raw ? 0 : 1) | (fixed ? 2 : 0));
   memcpy(o + 21, raw ? in : pl, pl_len);
   size_t w = 21 + pl_len;
   for (size_t b = 0; b < nbatches; b++) {
@@ -631,7 +694,13 @@ int co_compress(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelear
   return 0;
 }
 
-/* decompress (cucm_decompress_v2.cu:1185-1248). */
+int co_compress(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelearn, int batch, int threads,
+                uint8_t **out, size_t *out_n) {
+  return co_compress_ex(in, n, cs, unit, prelearn, batch, 0, threads, out, out_n);
+}
+
+/* decompress (cucm_decompress_v2.cu:1185-1248); flag bit 1 is the
+ * fixed-model variant. */
 int co_decompress(const uint8_t *in, size_t n, int threads, uint8_t **out, size_t *out_n) {
   tables_once();
   if (n < 21) return -3;
@@ -641,8 +710,9 @@ int co_decompress(const uint8_t *in, size_t n, int threads, uint8_t **out, size_
   size_t cs = get_be32(in + 8);
   size_t pl_coded = get_be32(in + 12);
   size_t prelearn = get_be32(in + 16);
-  int coded = in[20];
-  if (cs == 0 || unit <= 0 || batch <= 0 || prelearn > total) return -3;
+  int coded = in[20] & 1;
+  int fixed = (in[20] & 2) != 0;
+  if (cs == 0 || unit <= 0 || batch <= 0 || prelearn > total || (fixed && !prelearn)) return -3;
   size_t pl_len = coded ? pl_coded : prelearn;
   if (21 + pl_len > n) return -3;
   uint8_t *o = (uint8_t *)calloc(total ? total : 1, 1);
@@ -699,6 +769,7 @@ int co_decompress(const uint8_t *in, size_t n, int threads, uint8_t **out, size_
     J.cin_n = cin_n;
     J.dout = o + prelearn;
     J.decode = 1;
+    J.fixed = fixed;
     rc = run_jobs(&J, threads);
   }
   free(cin);

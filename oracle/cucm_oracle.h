@@ -69,7 +69,15 @@ void co_decode_chunk(co_model *work, const uint8_t *payload, size_t plen, size_t
  * one per online CPU.  Returns 0 or a negative error. */
 int co_compress(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelearn, int batch,
                 int threads, uint8_t **out, size_t *out_n);
-/* cucm_decompress_v2.cu:1185-1248. */
+/* The same with the fixed-model variant when `fixed` (PDF section 4.5: the
+ * prelearned model codes every chunk unchanged, data bits only; header flag
+ * bit 1; prelearn > 0 required).  co_compress is co_compress_ex(.., 0, ..). */
+int co_compress_ex(const uint8_t *in, size_t n, size_t cs, int unit, size_t prelearn, int batch, int fixed,
+                   int threads, uint8_t **out, size_t *out_n);
+/* One chunk of the fixed-model variant, and its inverse; m is only read. */
+size_t co_encode_chunk_fixed(const co_model *m, const uint8_t *chunk, size_t len, uint8_t *out, size_t cap);
+void co_decode_chunk_fixed(const co_model *m, const uint8_t *payload, size_t plen, size_t len, uint8_t *out);
+/* cucm_decompress_v2.cu:1185-1248 (and the fixed-model variant's flag). */
 int co_decompress(const uint8_t *in, size_t n, int threads, uint8_t **out, size_t *out_n);
 
 /* Upper bound on one chunk's payload for chunk size cs: every coded bit can

@@ -26,6 +26,9 @@ def lib():
     L.co_compress.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int, ctypes.c_size_t,
                               ctypes.c_int, ctypes.c_int, u8pp, ctypes.POINTER(ctypes.c_size_t)]
     L.co_compress.restype = ctypes.c_int
+    L.co_compress_ex.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int, ctypes.c_size_t,
+                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, u8pp, ctypes.POINTER(ctypes.c_size_t)]
+    L.co_compress_ex.restype = ctypes.c_int
     L.co_decompress.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, u8pp, ctypes.POINTER(ctypes.c_size_t)]
     L.co_decompress.restype = ctypes.c_int
     L.co_tables.argtypes = [ctypes.c_void_p] * 3
@@ -48,12 +51,14 @@ def _take(p, n):
     return out
 
 
-def compress(data, chunksize=1 << 20, unit=128, prelearn=0, batch=100, threads=0):
-    """Whole container, the reference's output for `cucm_compress -s -u -p -b`."""
+def compress(data, chunksize=1 << 20, unit=128, prelearn=0, batch=100, threads=0, fixed=False):
+    """Whole container, the reference's output for `cucm_compress -s -u -p -b`
+    (with `fixed`, the fixed-model variant of the paper's section 4.5)."""
     buf, n = _ptr(data)
     out = ctypes.POINTER(ctypes.c_uint8)()
     on = ctypes.c_size_t()
-    rc = lib().co_compress(buf, n, chunksize, unit, prelearn, batch, threads, ctypes.byref(out), ctypes.byref(on))
+    rc = lib().co_compress_ex(buf, n, chunksize, unit, prelearn, batch, 1 if fixed else 0, threads,
+                              ctypes.byref(out), ctypes.byref(on))
     if rc:
         raise RuntimeError("oracle compress failed: %d" % rc)
     return _take(out, on)
