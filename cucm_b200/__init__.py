@@ -366,9 +366,10 @@ class Context:
             raise CucmError(rc, "cucm_decompress")
         return buf.raw[:got.value]
 
-    def compress_dev(self, d_in, n, d_out, cap, chunksize=1 << 20, unit=128, prelearn=0, batch=100):
+    def compress_dev(self, d_in, n, d_out, cap, chunksize=1 << 20, unit=128, prelearn=0, batch=100,
+                     fmt=FORMAT_AUTO, fixed=False):
         """Device pointers in and out; returns the container size."""
-        p = default_params(chunksize, unit, prelearn, batch)
+        p = default_params(chunksize, unit, prelearn, batch, fmt, fixed)
         got = ctypes.c_uint64()
         rc = lib().cucm_compress_dev(self._h, d_in, n, ctypes.byref(p), d_out, cap, ctypes.byref(got))
         if rc:
