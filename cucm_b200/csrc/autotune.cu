@@ -89,7 +89,7 @@ extern "C" int cucm_autotune(cucm_ctx *c, const uint8_t *sample, uint64_t n, con
   // compressor: CTAs per SM in the persistent form; one chunk per launch in
   // the plain form
   for (int f = 0; f < 2; f++) {
-    const int lo = forms[f] == CUCM_FORM_PERSISTENT ? 1 : 0, hi = forms[f] == CUCM_FORM_PERSISTENT ? 3 : 0;
+    const int lo = forms[f] == CUCM_FORM_PERSISTENT ? 1 : 0, hi = forms[f] == CUCM_FORM_PERSISTENT ? 2 : 0;
     for (int k = lo; k <= hi; k++) {
       cucm_tune_result r = candidate(forms[f]);
       r.tuning.cmp_ctas = k;

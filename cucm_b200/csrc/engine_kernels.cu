@@ -589,12 +589,12 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
 }
 
 // Pipelined compressor CTAs that fit on one SM: shared memory (1 KiB of it
-// reserved per CTA by the hardware) and, at units <= 128 bits, the 96-register
-// cap that lets three share the register file.
+// reserved per CTA by the hardware) and the registers of two CTAs
+// (__launch_bounds__(kFastThreads, 2)).
 static int fast_ctas_per_sm(int unit) {
   const size_t per = make_fast_layout(unit).total + 1024 + 64;
   const int by_smem = (int)((228u * 1024u) / per);
-  const int by_regs = unit <= 128 ? 3 : 2;
+  const int by_regs = 2;
   const int n = by_smem < by_regs ? by_smem : by_regs;
   return n < 1 ? 1 : n;
 }

@@ -89,7 +89,7 @@ typedef struct cucm_tuning {
   int kernel;          /* 0 = pipelined kernels where the unit allows, 1 = generic kernels */
   int dec_pairs;       /* decoder chunks (warp pairs) per CTA, 0 = spread over all SMs first */
   int dec_tables;      /* decoder order 0/1 tables: 0 = shared memory where it fits, 1 = slot tables */
-  int cmp_ctas;        /* pipelined compressor CTAs (chunks) per SM, 1..3 (3 only at units <= 128); 0 = most that fit */
+  int cmp_ctas;        /* pipelined compressor CTAs (chunks) per SM, 1 or 2; 0 = most that fit */
   uint32_t dec_spin_limit; /* polls bounding the decoder's wait between its two warps; 0 = 2^27 (seconds).
                             * When a wait runs out the call returns CUCM_ETIMEOUT and the context stays
                             * usable; a small value makes that happen on purpose (tests). */
