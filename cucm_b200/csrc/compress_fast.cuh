@@ -412,11 +412,8 @@ CUCM_UNROLL
 // Chain (lane = order): StateMap probability updates of unit v in bit order.
 // A record is statep | dt[c] << 32 | dt[c+1] << 48 for the state's count c;
 // the count only ever grows by one per update, so a run of updates of one
-// state needs each table value two steps after it is requested.  The record
-// of the state two bits ahead is read a step early and the store of each
-// result is deferred by a step, so neither shared-memory round trip is on
-// the step-to-step chain: the record read one step ahead misses at most the
-// results of the two steps since, which are forwarded from registers.
+// state needs each table value two steps after it is requested, and the
+// record store is deferred by one step so it never waits for that load.
 __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &L, int o, int v, int n) {
   const int U = L.U;
   const uint8_t *sta = s.st + (v & 1) * U * kOrders + o;
@@ -425,37 +422,29 @@ __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &
   const uint16_t *dt = s.tab->dt;
   int st = sta[0];
   int st1 = n > 1 ? sta[kOrders] : 0;
-  int st2 = n > 2 ? sta[2 * kOrders] : 0;
   const uint64_t r0 = rec[st * kOrders];
-  uint64_t r1 = rec[st1 * kOrders];  // no result is pending yet
   uint32_t val = (uint32_t)r0, d = (uint32_t)(r0 >> 32) & 0xffffu, dn = (uint32_t)(r0 >> 48);
-  int pst = st;  // state of the previous step and its result (stored one step late)
+  int pst = st;
   uint64_t pnr = r0;
   uint32_t ywd = 0;
   for (int j = 0; j < n; j++) {
-    rec[pst * kOrders] = pnr;                  // the previous step's result
-    const uint64_t r2 = rec[st2 * kOrders];    // state j+2, as of the stores so far
-    const int st3 = (j + 3 < n) ? sta[(j + 3) * kOrders] : 0;
+    rec[pst * kOrders] = pnr;  // deferred store of the previous step
+    const uint64_t r1 = rec[st1 * kOrders];
+    const int st2 = (j + 2 < n) ? sta[(j + 2) * kOrders] : 0;
     if ((j & 31) == 0) ywd = yw[j >> 5];
     const uint32_t y = (ywd >> (j & 31)) & 1u;
     const uint32_t cnt = val & 1023u;
     const uint32_t dnn = dt[cnt < 1021u ? cnt + 2 : 1023u];
     const int32_t err = (int32_t)((y << 22) - (val >> 10));
     const uint32_t v2 = val + (((uint32_t)(err >> 3) * d) & 0xfffffc00u) + (cnt < 1023u ? 1u : 0u);
-    const uint64_t nr = (uint64_t)v2 | ((uint64_t)dn << 32) | ((uint64_t)dnn << 48);
-    // state j+1: this step's result, else the previous step's (r1 was read
-    // before that was stored), else r1
-    const uint64_t src = st1 == pst ? pnr : r1;
-    const bool fwd = st1 == st;
-    val = fwd ? v2 : (uint32_t)src;
-    d = fwd ? dn : (uint32_t)(src >> 32) & 0xffffu;
-    dn = fwd ? dnn : (uint32_t)(src >> 48);
     pst = st;
-    pnr = nr;
+    pnr = (uint64_t)v2 | ((uint64_t)dn << 32) | ((uint64_t)dnn << 48);
+    const bool fwd = st1 == st;
+    val = fwd ? v2 : (uint32_t)r1;
+    d = fwd ? dn : (uint32_t)(r1 >> 32) & 0xffffu;
+    dn = fwd ? dnn : (uint32_t)(r1 >> 48);
     st = st1;
     st1 = st2;
-    st2 = st3;
-    r1 = r2;
   }
   rec[pst * kOrders] = pnr;
 }

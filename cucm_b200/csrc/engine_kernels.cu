@@ -608,8 +608,6 @@ cudaError_t launch_compress(const ChunkTask *d_tasks, uint32_t ntasks, uint8_t *
     const void *kern = unit <= 128 ? (const void *)compress_fast_kernel : (const void *)compress_fast_kernel_wide;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
     if (unit <= 128)
       compress_fast_kernel<<<nslots, kFastThreads, smem, stream>>>(d_tasks, ntasks, slots, init_tables, d_init,
                                                                     d_queue, d_status, unit, tails, tail_count);
