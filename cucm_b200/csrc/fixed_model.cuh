@@ -125,19 +125,34 @@ __global__ void __launch_bounds__(128) fixed_coder_kernel(const FixedTask *tasks
   uint32_t x1 = 0, x2 = 0xffffffffu;
   uint64_t head = 0;
   const uint4 *src = reinterpret_cast<const uint4 *>(t.prm);
-  for (uint64_t q = 0; q < t.in_len; q++) {
-    const uint4 v = __ldg(src + q);
-    const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+  const uint64_t n = t.in_len;
+  // four bytes' inputs per group; the next group's loads are in flight
+  // while the current one is coded
+  uint4 nxt[4];
 CUCM_UNROLL
-    for (int h = 0; h < 8; h++) {
-      const uint32_t e = (w4[h >> 1] >> (16 * (h & 1))) & 0xffffu;
-      const uint32_t xm = x1 + __umulhi(x2 - x1, (e >> 1) << 20);
-      if (e & 1) x2 = xm; else x1 = xm + 1;
-      while ((x1 ^ x2) < 0x1000000u) {
-        if (head < t.out_cap) t.out[head] = (uint8_t)(x2 >> 24);
-        head++;
-        x1 <<= 8;
-        x2 = (x2 << 8) | 255u;
+  for (int b = 0; b < 4; b++) nxt[b] = (uint64_t)b < n ? __ldg(src + b) : make_uint4(0, 0, 0, 0);
+  for (uint64_t q = 0; q < n; q += 4) {
+    uint4 cur[4];
+CUCM_UNROLL
+    for (int b = 0; b < 4; b++) {
+      cur[b] = nxt[b];
+      nxt[b] = q + 4 + b < n ? __ldg(src + q + 4 + b) : make_uint4(0, 0, 0, 0);
+    }
+CUCM_UNROLL
+    for (int b = 0; b < 4; b++) {
+      if (q + b >= n) break;
+      const uint32_t w4[4] = {cur[b].x, cur[b].y, cur[b].z, cur[b].w};
+CUCM_UNROLL
+      for (int h = 0; h < 8; h++) {
+        const uint32_t e = (w4[h >> 1] >> (16 * (h & 1))) & 0xffffu;
+        const uint32_t xm = x1 + __umulhi(x2 - x1, (e >> 1) << 20);
+        if (e & 1) x2 = xm; else x1 = xm + 1;
+        while ((x1 ^ x2) < 0x1000000u) {
+          if (head < t.out_cap) t.out[head] = (uint8_t)(x2 >> 24);
+          head++;
+          x1 <<= 8;
+          x2 = (x2 << 8) | 255u;
+        }
       }
     }
   }
