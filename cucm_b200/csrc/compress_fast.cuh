@@ -43,14 +43,10 @@ constexpr int kWinBytes = kFastMaxUnit / 8 + 8;    // input window of a unit (+7
 
 constexpr int kFastStageMin = 2048;
 
-// The tables a compress CTA keeps in shared memory: the adaptation rates of
-// the chain and the state machine of the walker.  Stretch and squash are read
-// through the read-only cache from the device copy instead, which the SM's
-// CTAs share: that is what lets three CTAs share an SM at units <= 128.
-struct FastTables {
-  uint16_t dt[1024];
-  uint8_t nex[256][2];
-};
+// A compress CTA keeps the whole of the tables in shared memory (reading
+// stretch and squash through the read-only cache instead measured 10 %
+// slower: the lookups are on the front warps' critical path).
+typedef Tables FastTables;
 
 struct FastLayout {
   int U, NSLOT, NBK, logNBK, stage;
@@ -136,23 +132,6 @@ __device__ inline FastSmem carve_fast(uint8_t *b, const FastLayout &L) {
   return s;
 }
 
-// Mixer output for one bit (Mixer::p, cucm_compress_v2.cu:636-644, then
-// `if (pr < 2048) pr++`), squash read through the read-only cache.
-__device__ __forceinline__ int mix_pr_ro(const int32_t *w, int cxt, const int smp[kOrders]) {
-  long long sum = 0;
-CUCM_UNROLL
-  for (int o = 0; o < kOrders; o++) sum += (long long)w[cxt * kOrders + o] * smp[o];
-  sum >>= 16;
-  const int idx = sum < -2047 ? -2047 : (sum > 2048 ? 2048 : (int)sum);
-  const int pr = __ldg(&g_tables.squash[idx + 2047]);
-  return pr < 2048 ? pr + 1 : pr;
-}
-
-__device__ inline void copy_fast_tables(FastTables *dst) {
-  for (int i = threadIdx.x; i < 1024; i += blockDim.x) dst->dt[i] = g_tables.dt[i];
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) (&dst->nex[0][0])[i] = (&g_tables.nex[0][0])[i];
-}
-
 __device__ __forceinline__ void named_barrier(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
@@ -226,44 +205,13 @@ __device__ __forceinline__ int slot_find(const uint32_t *row, int logNBK, uint32
 }
 
 // Front: slots of unit v in its own table, and in the previous unit's.
-// Front warp w owns orders 2w and 2w + 1, so no other warp touches their
-// rows.  Each lane inserts its keys (bits lane, lane + 32, ... of both
-// orders) with shared-memory compare-and-swap, four keys at a time so their
-// round trips overlap: read the key's bucket; a hit is the key's slot,
-// otherwise CAS the key into the bucket's first free place.  A CAS that finds
-// the same key there shares its slot; one that finds another key re-reads
-// the bucket.  Places fill in order and are never emptied within a unit, so
-// every key ends in exactly one place whichever lane inserts it first; a
-// full bucket spills to the next one.  The previous unit's table is only
-// read (the link of each key).
-
-// A bucket's four keys, read from shared memory as they are now (other lanes
-// may have inserted since an earlier read).
-__device__ __forceinline__ uint4 ld_bucket(const uint32_t *p) {
-  uint4 v;
-  asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "r"((uint32_t)__cvta_generic_to_shared(p)));
-  return v;
-}
-
-__device__ __forceinline__ int slot_insert(uint32_t *row, uint32_t b, uint32_t nbk_mask, uint32_t kp, uint4 q) {
-  for (;;) {
-    if (q.x == kp) return 4 * b;
-    if (q.y == kp) return 4 * b + 1;
-    if (q.z == kp) return 4 * b + 2;
-    if (q.w == kp) return 4 * b + 3;
-    const int used = (q.x != 0) + (q.y != 0) + (q.z != 0) + (q.w != 0);
-    if (used < 4) {
-      const uint32_t old = atomicCAS(row + 4 * b + used, 0u, kp);
-      if (old == 0u || old == kp) return 4 * b + used;
-    } else {
-      b = (b + 1) & nbk_mask;
-    }
-    q = ld_bucket(row + 4 * b);
-  }
-}
-
+// Front warp w owns orders 2w and 2w + 1, so no other warp writes its rows;
+// a step takes two bytes, lane = (order, bit, byte).  A lane whose key is
+// not yet in the table either follows a lane of the step with the same key
+// (a slot recurs at most once per byte) or, as the key's leader, takes the
+// next free place of its bucket after the leaders before it in the same
+// bucket (warp match and rank, no atomics).  Leaders that find their bucket
+// full move on to the next bucket and rank again.
 __device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
   const int U = L.U, NS = L.NSLOT;
   uint32_t *hk = s.hk + (v & 1) * kOrders * NS;
@@ -272,6 +220,9 @@ __device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout 
   uint16_t *lnk = s.lnk + (v & 1) * kOrders * U;
   uint16_t *bkt = s.bkt + (v & 1) * kOrders * U;
   const int lane = t & 31, w = t >> 5;
+  const int o = 2 * w + (lane >> 4), r = (lane >> 1) & 7, half = lane & 1;
+  uint32_t *row = hk + o * NS;
+  const uint32_t *prow = hk_prev + o * NS;
   const uint32_t nbk_mask = (uint32_t)L.NSLOT / 4 - 1;
   {
     // this warp's two rows
@@ -280,56 +231,56 @@ __device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout 
     for (int i = lane; i < 2 * NS / 4; i += 32) k4[i] = z;
     __syncwarp();
   }
-  // key i of this lane: order 2w + (i & 1), bit lane + 32 * (2g + (i >> 1))
-  for (int g = 0; 64 * g < nvalid; g++) {
-    uint32_t kp[4], b[4];
-    int idx[4];
-    uint4 q[4];
-CUCM_UNROLL
-    for (int i = 0; i < 4; i++) {
-      const int j = lane + 32 * (2 * g + (i >> 1)), o = 2 * w + (i & 1);
-      idx[i] = j * kOrders + o;
-      kp[i] = j < nvalid ? key[idx[i]] + 1 : 0u;
-      b[i] = bucket_of(kp[i] - 1, L.logNBK);
-    }
-CUCM_UNROLL
-    for (int i = 0; i < 4; i++)
-      if (kp[i]) q[i] = ld_bucket(hk + (2 * w + (i & 1)) * NS + 4 * b[i]);
-    // a hit, or one CAS into the first free place, for all four at once
-    int sl[4], pos[4];
-    uint32_t old[4];
-CUCM_UNROLL
-    for (int i = 0; i < 4; i++) {
-      sl[i] = -1;
-      pos[i] = -1;
-      old[i] = 0u;
-      if (!kp[i]) continue;
-      const uint4 x = q[i];
-      const int hit = x.x == kp[i] ? 0 : x.y == kp[i] ? 1 : x.z == kp[i] ? 2 : x.w == kp[i] ? 3 : -1;
-      const int used = (x.x != 0) + (x.y != 0) + (x.z != 0) + (x.w != 0);
-      if (hit >= 0) {
-        sl[i] = 4 * (int)b[i] + hit;
-      } else if (used < 4) {
-        pos[i] = 4 * (int)b[i] + used;
-        old[i] = atomicCAS(hk + (2 * w + (i & 1)) * NS + pos[i], 0u, kp[i]);
+  const unsigned lt = (1u << lane) - 1u;
+  for (int q0 = 0; q0 < (nvalid >> 3); q0 += 2) {
+    const int q = q0 + half;
+    const bool valid = q < (nvalid >> 3);
+    const int idx = (q * 8 + r) * kOrders + o;
+    const uint32_t kp = valid ? key[idx] + 1 : 0u;
+    // cross-unit link: the previous unit's table is read-only here
+    if (valid) lnk[idx] = (uint16_t)(slot_find(prow, L.logNBK, kp) + 1);
+    // this unit's slot
+    uint32_t b = bucket_of(kp - 1, L.logNBK);
+    int slot_id = -1;
+    bool pending = valid;
+    // lanes with the same key (and order) in this step share one slot
+    const unsigned same = __match_any_sync(0xffffffffu, valid ? ((uint32_t)o << 25 | (kp - 1)) : 0xffffffffu);
+    const bool leader = valid && (same & lt) == 0;
+    const int lead = __ffs(same) - 1;
+    while (__any_sync(0xffffffffu, pending)) {
+      uint4 qb = make_uint4(1, 1, 1, 1);
+      if (pending) qb = *reinterpret_cast<const uint4 *>(row + 4 * b);
+      if (pending) {
+        if (qb.x == kp) slot_id = 4 * b;
+        else if (qb.y == kp) slot_id = 4 * b + 1;
+        else if (qb.z == kp) slot_id = 4 * b + 2;
+        else if (qb.w == kp) slot_id = 4 * b + 3;
+        if (slot_id >= 0) pending = false;
+      }
+      // leaders still without a slot claim a free place of their bucket
+      const bool claim = pending && leader;
+      const unsigned mb = __match_any_sync(0xffffffffu, claim ? ((uint32_t)o << 8 | b) : 0xffffffffu);
+      if (claim) {
+        const int used = (qb.x != 0) + (qb.y != 0) + (qb.z != 0) + (qb.w != 0);
+        const int pos = used + __popc(mb & lt);
+        if (pos < 4) {
+          row[4 * b + pos] = kp;
+          slot_id = 4 * b + pos;
+          pending = false;
+        } else {
+          b = (b + 1) & nbk_mask;
+        }
+      }
+      __syncwarp();
+      // followers take their leader's slot once it has one
+      const int ls = __shfl_sync(0xffffffffu, slot_id, lead);
+      if (pending && !leader && ls >= 0) {
+        slot_id = ls;
+        pending = false;
       }
     }
-CUCM_UNROLL
-    for (int i = 0; i < 4; i++) {
-      if (!kp[i]) continue;
-      const int o = 2 * w + (i & 1);
-      if (sl[i] < 0 && pos[i] >= 0 && (old[i] == 0u || old[i] == kp[i])) sl[i] = pos[i];
-      if (sl[i] < 0) {  // lost the place to another key, or the bucket is full
-        const uint32_t bb = pos[i] >= 0 ? b[i] : ((b[i] + 1) & nbk_mask);
-        sl[i] = slot_insert(hk + o * NS, bb, nbk_mask, kp[i], ld_bucket(hk + o * NS + 4 * bb));
-      }
-      bkt[idx[i]] = (uint16_t)sl[i];
-    }
-CUCM_UNROLL
-    for (int i = 0; i < 4; i++)
-      if (kp[i]) lnk[idx[i]] = (uint16_t)(slot_find(hk_prev + (2 * w + (i & 1)) * NS, L.logNBK, kp[i]) + 1);
+    if (valid) bkt[idx] = (uint16_t)slot_id;
   }
-  __syncwarp();
 }
 
 // Walker: bit-history updates of unit v in bit order, a byte per step.  A
@@ -476,7 +427,7 @@ __device__ __forceinline__ void front_mix(const FastSmem &s, const FastLayout &L
           olen += (sm != 1);
         }
         const int cx = olen + (c1[j >> 3] >> 5) * 10;
-        const int pr = mix_pr_ro(s.w, cx, smps[h]);
+        const int pr = mix_pr(s.w, cx, smps[h], s.tab);
         const int y = (yw[j >> 5] >> (j & 31)) & 1;
         prm[j] = (uint16_t)((pr << 1) | y);
         cxs[h] = cx;
@@ -593,7 +544,7 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
       if (um >= 0 && um < nU) {
         const int k = warp == kWChain ? lane : 32 + ft;
         for (int i = k; i < kOrders * 256; i += kSnapThreads)
-          s.snap[i] = __ldg(&g_tables.stretch[(uint32_t)s.rec[i] >> 20]);
+          s.snap[i] = s.tab->stretch[(uint32_t)s.rec[i] >> 20];
       }
       named_barrier(1, kSnapThreads);
     }
@@ -680,7 +631,7 @@ __device__ __forceinline__ void compress_fast_loop(const ChunkTask *tasks, uint3
   const FastLayout L = make_fast_layout(unit);
   const FastSmem s = carve_fast(smem_raw, L);
   uint8_t *slot = slots + (size_t)blockIdx.x * kSlotTableBytes;
-  copy_fast_tables(s.tab);
+  copy_tables(&g_tables, s.tab);
   __shared__ uint32_t s_task;
   bool fresh = true;
   for (;;) {
@@ -731,7 +682,7 @@ __global__ void __launch_bounds__(kFastThreads, 2)
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const FastLayout L = make_fast_layout((int)t.unit);
   const FastSmem s = carve_fast(smem_raw, L);
-  copy_fast_tables(s.tab);
+  copy_tables(&g_tables, s.tab);
   __syncthreads();
   compress_fast_one<GR>(t, slot, s, L, init, status, nullptr, nullptr);
 }

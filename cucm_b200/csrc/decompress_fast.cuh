@@ -314,12 +314,10 @@ CUCM_UNROLL
   }
 }
 
-// Unit end, both warps of the pair (t = 0..63): overlay -> slot tables,
-// live probabilities become frozen (stretched for the mixer), deltas join
-// the weights, the unit's bytes go out.  Called between two pair barriers.
-// The overlay is left in place: the decoding warp looks the next unit's
-// first keys up in it at the same time (dec_overlay_fix), and the updating
-// warp clears it after the second barrier (dec_overlay_clear).
+// Unit end, both warps of the pair (t = 0..63): overlay -> slot tables (and
+// cleared), live probabilities become frozen (stretched for the mixer),
+// deltas join the weights, the unit's bytes go out.  Called between two pair
+// barriers.
 __device__ inline void dec_unit_end(const DecSmem &s, const DecLayout &L, const Tables *tab, uint8_t *slot,
                                     uint8_t *out, int nbytes, int t) {
 CUCM_UNROLL
@@ -330,6 +328,7 @@ CUCM_UNROLL
       const int b = s.ovl[e * kOrders + o];
       const uint32_t kk = s.ovk[o * L.NS + b];
       tb[kk - 1] = s.ovs[o * L.NS + b];
+      s.ovk[o * L.NS + b] = 0;
     }
   }
   const uint4 *src = reinterpret_cast<const uint4 *>(s.spl);
@@ -355,39 +354,6 @@ CUCM_UNROLL
     d4[i] = make_int4(0, 0, 0, 0);
   }
   if (t < nbytes) out[t] = s.outb[t];
-}
-
-// The unit's overlay entries emptied for the next unit (the updating warp,
-// lane = order, after the unit end).
-__device__ __forceinline__ void dec_overlay_clear(const DecSmem &s, const DecLayout &L, int lane) {
-  if (lane < kOrders) {
-    const int n = s.ovn[lane];
-    for (int e = 0; e < n; e++) s.ovk[lane * L.NS + s.ovl[e * kOrders + lane]] = 0;
-  }
-  __syncwarp();
-}
-
-// The next unit's first gathers go out before the unit end has written the
-// overlay back; a key the overlay holds takes its state from there.
-__device__ __forceinline__ void dec_overlay_fix(const DecSmem &s, const DecLayout &L, const BitKeys &kk,
-                                                uint32_t st[kOrders]) {
-  const uint32_t bmask = (uint32_t)(L.NS / 4 - 1);
-CUCM_UNROLL
-  for (int o = 0; o < kOrders; o++) {
-    const uint32_t want = kk.k[o] + 1;
-    const uint4 *ovk4 = reinterpret_cast<const uint4 *>(s.ovk + o * L.NS);
-    uint32_t b = bucket_of(kk.k[o], L.logNS - 2);
-    for (uint32_t it = 0; it <= bmask; it++) {
-      const uint4 q = ovk4[b];
-      const int h = bucket_place(q, want);
-      if (h >= 0) {
-        st[o] = s.ovs[o * L.NS + 4 * b + (uint32_t)h];
-        break;
-      }
-      if (bucket_used(q) < 4) break;
-      b = (b + 1) & bmask;
-    }
-  }
 }
 
 // The pair's barrier: named barrier 1 + pair index, 64 threads.
@@ -452,7 +418,6 @@ __device__ void decompress_pair_one(const ChunkTask &t, uint8_t *slot, const Dec
       pair_sync(pair);
       dec_unit_end(s, L, tab, slot, t.out + (base >> 3), nunit >> 3, t64);
       pair_sync(pair);
-      dec_overlay_clear(s, L, lane);
     }
     return;
   }
@@ -493,12 +458,11 @@ CUCM_UNROLL
     for (int o = kLow ? 2 : 0; o < kOrders; o++) sv[o] = ld_slot_state(slot + table_offset(o) + k.k[o]);
   };
 
-  if (nbits) gather(kk, st, cur, r, hist);
   for (uint64_t base = 0; base < nbits; base += (uint64_t)U) {
     const int nunit = (int)(nbits - base < (uint64_t)U ? nbits - base : (uint64_t)U);
     const int nr = nunit >> 2;
-    const bool more = base + (uint64_t)U < nbits;
     int obyte = 0;
+    gather(kk, st, cur, r, hist);
     for (int rd = 0; rd < nr; rd++) {
       if ((long long)ioff + 16 > wbase + kDecWin) wbase = dec_refill(s.win, pay, plen, ioff, lane);
       // stretch, mixer context, mixer output (cucm_decompress_v2.cu:774-809)
@@ -560,9 +524,7 @@ CUCM_UNROLL
         cur = 0;
         r = 0;
       }
-      // the next round's gathers; past the unit's last round, the next
-      // unit's first (corrected from the overlay at the unit end)
-      if (rd + 1 < nr || more) gather(kk, st, cur, r, hist);
+      if (rd + 1 < nr) gather(kk, st, cur, r, hist);
       // the path's lanes record their bit for the updating warp
       if (on_path) {
         const int i = depth;
@@ -585,7 +547,6 @@ CUCM_UNROLL
       }
     }
     pair_sync(pair);
-    if (more) dec_overlay_fix(s, L, kk, st);
     dec_unit_end(s, L, tab, slot, t.out + (base >> 3), nunit >> 3, t64);
     pair_sync(pair);
   }
