@@ -564,17 +564,21 @@ cudaError_t launch_fixed_encode(const FixedTask *d_tasks, const uint64_t *d_firs
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  fixed_coder_kernel<<<(ntasks + 127) / 128, 128, 0, stream>>>(d_tasks, ntasks, d_status);
+  // one warp of coders per CTA: the warps land on different SMs
+  fixed_coder_kernel<<<(ntasks + 31) / 32, 32, 0, stream>>>(d_tasks, ntasks, d_status);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fixed_decode(const FixedTask *d_tasks, uint32_t ntasks, const uint8_t *image,
                                 const ModelInit *d_init, uint32_t *d_queue, int sm_count, cudaStream_t stream) {
   if (ntasks == 0) return cudaSuccess;
-  const uint32_t want = (ntasks + kFixedDecWarps - 1) / kFixedDecWarps;
-  const uint32_t cap = (uint32_t)(sm_count > 0 ? sm_count : 148) * 4;
-  fixed_decode_kernel<<<std::min(want, cap), kFixedDecWarps * 32, 0, stream>>>(d_tasks, ntasks, image, d_init,
-                                                                              d_queue);
+  // chunks spread over all SMs first: warps per CTA = chunks per SM, at
+  // most kFixedDecWarps (each warp's rounds wait on its gathers, so warps
+  // sharing an SM slow each other only through its load pipe)
+  const uint32_t sms = (uint32_t)(sm_count > 0 ? sm_count : 148);
+  const uint32_t warps = std::min<uint32_t>(kFixedDecWarps, (ntasks + sms - 1) / sms);
+  const uint32_t want = (ntasks + warps - 1) / warps;
+  fixed_decode_kernel<<<std::min(want, sms * 4), warps * 32, 0, stream>>>(d_tasks, ntasks, image, d_init, d_queue);
   return cudaGetLastError();
 }
 

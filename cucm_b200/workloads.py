@@ -117,6 +117,19 @@ def _derive(seed, i):
     return int(np.random.SeedSequence([seed, i]).generate_state(1, dtype=np.uint64)[0])
 
 
+def long_text(total, seed, piece=4 << 20):
+    """`total` bytes of the Markov text in `piece`-byte pieces, each its own
+    seeded walk of the same language, generated on host threads."""
+    out = np.empty(total, dtype=np.uint8)
+
+    def fill(i):
+        a = i * piece
+        out[a:a + piece] = text(min(piece, total - a), _derive(seed, i))
+
+    _parallel(fill, range((total + piece - 1) // piece))
+    return out
+
+
 def config0():
     """1 MiB of Markov text; 64 KiB chunks (16 chunks)."""
     return text(1 << 20, _derive(0, 0)), dict(chunksize=64 << 10, unit=128, prelearn=0, batch=100)
