@@ -12,10 +12,9 @@
 //     are free.  Requests that arrive while others run are admitted as soon
 //     as slots free up -- there is no waiting for the GPU to drain;
 //   * a launch takes all admissible requests of one kind (operation, unit
-//     length, no prelearn model) and size class (chunk counts within a
-//     factor of four) and runs every chunk of them in one persistent engine
-//     launch on its own stream, over a contiguous run of slots; launches on
-//     different streams overlap on the device;
+//     length, no prelearn model) and runs every chunk of them in one
+//     persistent engine launch on its own stream, over a contiguous run of
+//     slots; launches on different streams overlap on the device;
 //   * compress launches finish in a second step: the payload lengths come
 //     back, the container layout is computed on the host, one pack kernel
 //     writes every container and the bytes go back to the caller;
@@ -597,26 +596,15 @@ void admit(cucm_server *s) {
       s->cv_done.notify_all();
       continue;
     }
-    // the head of the queue and every later request of its kind and size
-    // class (chunk count within a factor of four) that fits; the others get
-    // launches of their own, which overlap on the device -- so a small
-    // request does not wait for a large one's launch to finish
+    // the head of the queue and every later request of its kind that fits;
+    // other kinds wait for the next launch
     Req *h = cand[0];
     std::vector<Req *> grp{h};
     uint64_t need_slots = h->nchunks, bytes = req_bytes(h);
-    auto size_class = [](uint64_t nch) {
-      int c = 0;
-      while (nch > 1) {
-        nch >>= 2;
-        c++;
-      }
-      return c;
-    };
     if (!h->hm) {
       for (size_t j = 1; j < cand.size(); j++) {
         Req *r = cand[j];
         if (r->op != h->op || r->unit != h->unit || r->hm) continue;
-        if (size_class(r->nchunks) != size_class(h->nchunks)) continue;
         const uint64_t b = req_bytes(r);
         if (s->buf_used + bytes + b > s->buf_limit) break;
         grp.push_back(r);
