@@ -49,7 +49,7 @@ constexpr int kFastStageMin = 2048;
 typedef Tables FastTables;
 
 struct FastLayout {
-  int U, NSLOT, NBK, logNBK, stage;
+  int U, NSLOT, stage;
   size_t off_tab, off_rec, off_snap, off_w, off_hk, off_ns, off_key, off_lnk, off_bkt, off_fsw, off_st, off_fr,
       off_yw, off_c1, off_prm, off_win, off_stage, total;
 };
@@ -57,9 +57,7 @@ struct FastLayout {
 __host__ __device__ inline FastLayout make_fast_layout(int U) {
   FastLayout L;
   L.U = U;
-  L.NSLOT = next_pow2(2 * U);   // hash slots per order and unit (load <= 1/2)
-  L.NBK = L.NSLOT / 4;          // 4-slot buckets, one 16-byte load each
-  L.logNBK = ilog2(L.NBK);
+  L.NSLOT = U <= 128 ? 128 : 256;  // slots per order and unit: the keys sorted in 4 or 8 per lane
   L.stage = next_pow2(4 * U + 1024);  // a unit codes at most 4U bytes; flushes go out in 512-byte blocks
   if (L.stage < kFastStageMin) L.stage = kFastStageMin;
   const size_t NS = (size_t)L.NSLOT;
@@ -73,7 +71,7 @@ __host__ __device__ inline FastLayout make_fast_layout(int U) {
   L.off_rec = take(sizeof(uint64_t) * kOrders * 256);
   L.off_snap = take(sizeof(int16_t) * kOrders * 256);
   L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);
-  L.off_hk = take(sizeof(uint32_t) * 2 * kOrders * NS);    // slot keys + 1, [unit parity][order][slot]
+  L.off_hk = take(sizeof(uint32_t) * 2 * kOrders * NS);    // keys + 1 by slot, ascending [unit parity][order][slot]
   L.off_ns = take(sizeof(uint16_t) * 2 * kOrders * NS);    // 0x100 | state once written in the unit
   L.off_key = take(sizeof(uint32_t) * 2 * kOrders * U);    // [unit parity][bit][order]
   L.off_lnk = take(sizeof(uint16_t) * 2 * kOrders * U);    // slot + 1 in the previous unit's table, or 0
@@ -187,99 +185,128 @@ __device__ __forceinline__ void front_keys(const FastSmem &s, const FastLayout &
   }
 }
 
-// Slot tables: per order, NSLOT/4 buckets of 4 keys (key + 1, 0 = empty),
-// probed with one 16-byte load per bucket; a full bucket spills to the next.
-// Slot of key kp (key + 1) in a table, or -1.
-__device__ __forceinline__ int slot_find(const uint32_t *row, int logNBK, uint32_t kp) {
-  const uint32_t nbk_mask = (1u << logNBK) - 1u;
-  uint32_t b = bucket_of(kp - 1, logNBK);
-  for (;;) {
-    const uint4 q = *reinterpret_cast<const uint4 *>(row + 4 * b);
-    if (q.x == kp) return 4 * b;
-    if (q.y == kp) return 4 * b + 1;
-    if (q.z == kp) return 4 * b + 2;
-    if (q.w == kp) return 4 * b + 3;
-    if (q.x == 0 || q.y == 0 || q.z == 0 || q.w == 0) return -1;
-    b = (b + 1) & nbk_mask;
+// Slot tables: per order and unit, the unit's distinct keys (key + 1) in
+// ascending order, padded with kNoKey; a key's slot is its rank.  Sorting
+// the unit's keys once replaces a hash table built step by step (a claim
+// loop with a shared-memory round trip and a warp barrier per two bytes).
+constexpr uint32_t kNoKey = 0xffffffffu;
+
+// Ascending bitonic sort of 32 * E values, value p = lane * E + i in a[i]
+// of lane `lane`: distances below E are compare-swaps within a lane, the
+// others exchange with lane ^ (distance / E) by shuffle.
+template <int E>
+__device__ __forceinline__ void warp_sort(uint32_t (&a)[E], int lane) {
+  constexpr int N = 32 * E;
+  CUCM_UNROLL
+  for (int k = 2; k <= N; k <<= 1) {
+    CUCM_UNROLL
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= E) {
+        const int lm = j / E;
+        const bool lower = (lane & lm) == 0;
+        CUCM_UNROLL
+        for (int i = 0; i < E; i++) {
+          const uint32_t o = __shfl_xor_sync(0xffffffffu, a[i], lm);
+          const bool up = ((lane * E + i) & k) == 0;
+          a[i] = (up == lower) ? min(a[i], o) : max(a[i], o);
+        }
+      } else {
+        CUCM_UNROLL
+        for (int i = 0; i < E; i++) {
+          if ((i & j) == 0) {
+            const bool up = ((lane * E + i) & k) == 0;
+            const uint32_t x = a[i], y = a[i | j];
+            a[i] = up ? min(x, y) : max(x, y);
+            a[i | j] = up ? max(x, y) : min(x, y);
+          }
+        }
+      }
+    }
   }
 }
 
+// Position of kp in an ascending row of P (a power of two) entries, if it
+// is there: the returned position holds kp exactly when it is present.
+template <int P>
+__device__ __forceinline__ int row_find(const uint32_t *row, uint32_t kp) {
+  int lo = 0;
+  CUCM_UNROLL
+  for (int step = P >> 1; step > 0; step >>= 1) lo += row[lo + step - 1] < kp ? step : 0;
+  return lo;
+}
+
 // Front: slots of unit v in its own table, and in the previous unit's.
-// Front warp w owns orders 2w and 2w + 1, so no other warp writes its rows;
-// a step takes two bytes, lane = (order, bit, byte).  A lane whose key is
-// not yet in the table either follows a lane of the step with the same key
-// (a slot recurs at most once per byte) or, as the key's leader, takes the
-// next free place of its bucket after the leaders before it in the same
-// bucket (warp match and rank, no atomics).  Leaders that find their bucket
-// full move on to the next bucket and rank again.
+// Front warp w owns orders 2w and 2w + 1, so no other warp writes their
+// rows.  Per order: the unit's keys (bit j = lane + 32 i) are sorted across
+// the warp, the distinct ones written in order, then every bit finds its
+// key's rank in this unit's row (bkt) and in the previous unit's (lnk =
+// rank + 1, or 0 when the key was not touched there).  E keys per lane:
+// 32 * E >= U, and NSLOT = 32 * E.
+template <int E>
 __device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
-  const int U = L.U, NS = L.NSLOT;
-  uint32_t *hk = s.hk + (v & 1) * kOrders * NS;
-  const uint32_t *hk_prev = s.hk + ((v + 1) & 1) * kOrders * NS;
+  constexpr int P = 32 * E;
+  const int U = L.U;
   const uint32_t *key = s.key + (v & 1) * kOrders * U;
   uint16_t *lnk = s.lnk + (v & 1) * kOrders * U;
   uint16_t *bkt = s.bkt + (v & 1) * kOrders * U;
   const int lane = t & 31, w = t >> 5;
-  const int o = 2 * w + (lane >> 4), r = (lane >> 1) & 7, half = lane & 1;
-  uint32_t *row = hk + o * NS;
-  const uint32_t *prow = hk_prev + o * NS;
-  const uint32_t nbk_mask = (uint32_t)L.NSLOT / 4 - 1;
-  {
-    // this warp's two rows
-    uint4 *k4 = reinterpret_cast<uint4 *>(hk + 2 * w * NS);
-    const uint4 z = make_uint4(0, 0, 0, 0);
-    for (int i = lane; i < 2 * NS / 4; i += 32) k4[i] = z;
-    __syncwarp();
+  uint32_t kp[2][E], a[2][E];
+  CUCM_UNROLL
+  for (int h = 0; h < 2; h++) {
+    const int o = 2 * w + h;
+    CUCM_UNROLL
+    for (int i = 0; i < E; i++) {
+      const int j = lane + 32 * i;
+      kp[h][i] = j < nvalid ? key[j * kOrders + o] + 1 : kNoKey;
+      a[h][i] = kp[h][i];
+    }
   }
-  const unsigned lt = (1u << lane) - 1u;
-  for (int q0 = 0; q0 < (nvalid >> 3); q0 += 2) {
-    const int q = q0 + half;
-    const bool valid = q < (nvalid >> 3);
-    const int idx = (q * 8 + r) * kOrders + o;
-    const uint32_t kp = valid ? key[idx] + 1 : 0u;
-    // cross-unit link: the previous unit's table is read-only here
-    if (valid) lnk[idx] = (uint16_t)(slot_find(prow, L.logNBK, kp) + 1);
-    // this unit's slot
-    uint32_t b = bucket_of(kp - 1, L.logNBK);
-    int slot_id = -1;
-    bool pending = valid;
-    // lanes with the same key (and order) in this step share one slot
-    const unsigned same = __match_any_sync(0xffffffffu, valid ? ((uint32_t)o << 25 | (kp - 1)) : 0xffffffffu);
-    const bool leader = valid && (same & lt) == 0;
-    const int lead = __ffs(same) - 1;
-    while (__any_sync(0xffffffffu, pending)) {
-      uint4 qb = make_uint4(1, 1, 1, 1);
-      if (pending) qb = *reinterpret_cast<const uint4 *>(row + 4 * b);
-      if (pending) {
-        if (qb.x == kp) slot_id = 4 * b;
-        else if (qb.y == kp) slot_id = 4 * b + 1;
-        else if (qb.z == kp) slot_id = 4 * b + 2;
-        else if (qb.w == kp) slot_id = 4 * b + 3;
-        if (slot_id >= 0) pending = false;
-      }
-      // leaders still without a slot claim a free place of their bucket
-      const bool claim = pending && leader;
-      const unsigned mb = __match_any_sync(0xffffffffu, claim ? ((uint32_t)o << 8 | b) : 0xffffffffu);
-      if (claim) {
-        const int used = (qb.x != 0) + (qb.y != 0) + (qb.z != 0) + (qb.w != 0);
-        const int pos = used + __popc(mb & lt);
-        if (pos < 4) {
-          row[4 * b + pos] = kp;
-          slot_id = 4 * b + pos;
-          pending = false;
-        } else {
-          b = (b + 1) & nbk_mask;
-        }
-      }
-      __syncwarp();
-      // followers take their leader's slot once it has one
-      const int ls = __shfl_sync(0xffffffffu, slot_id, lead);
-      if (pending && !leader && ls >= 0) {
-        slot_id = ls;
-        pending = false;
+  warp_sort<E>(a[0], lane);
+  warp_sort<E>(a[1], lane);
+  CUCM_UNROLL
+  for (int h = 0; h < 2; h++) {
+    uint32_t *row = s.hk + ((v & 1) * kOrders + 2 * w + h) * P;
+    // distinct keys: a value is the first of its run unless it equals the
+    // one before it (the previous lane's last for i = 0)
+    const uint32_t before = __shfl_up_sync(0xffffffffu, a[h][E - 1], 1);
+    unsigned heads = 0;
+    CUCM_UNROLL
+    for (int i = 0; i < E; i++) {
+      const uint32_t prev = i ? a[h][i - 1] : before;
+      if (a[h][i] != kNoKey && (lane * E + i == 0 || a[h][i] != prev)) heads |= 1u << i;
+    }
+    const int cnt = __popc(heads);
+    int incl = cnt;
+    CUCM_UNROLL
+    for (int d = 1; d < 32; d <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += y;
+    }
+    const int nd = __shfl_sync(0xffffffffu, incl, 31);
+    int at = incl - cnt;
+    CUCM_UNROLL
+    for (int i = 0; i < E; i++) {
+      if (heads >> i & 1u) row[at++] = a[h][i];
+      const int q = lane * E + i;
+      if (q >= nd) row[q] = kNoKey;
+    }
+  }
+  __syncwarp();
+  CUCM_UNROLL
+  for (int h = 0; h < 2; h++) {
+    const int o = 2 * w + h;
+    const uint32_t *row = s.hk + ((v & 1) * kOrders + o) * P;
+    const uint32_t *prow = s.hk + (((v + 1) & 1) * kOrders + o) * P;
+    CUCM_UNROLL
+    for (int i = 0; i < E; i++) {
+      const int j = lane + 32 * i;
+      if (j < nvalid) {
+        const int d = row_find<P>(row, kp[h][i]);
+        const int pd = row_find<P>(prow, kp[h][i]);
+        bkt[j * kOrders + o] = (uint16_t)d;
+        lnk[j * kOrders + o] = (uint16_t)(prow[pd] == kp[h][i] ? pd + 1 : 0);
       }
     }
-    if (valid) bkt[idx] = (uint16_t)slot_id;
   }
 }
 
@@ -528,7 +555,7 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
       front_keys(s, L, ft, v, fast_nvalid(data_bits, U, v));
       front_sync();
     }
-    front_links(s, L, ft, 0, fast_nvalid(data_bits, U, 0));
+    front_links<GR / 2>(s, L, ft, 0, fast_nvalid(data_bits, U, 0));
     front_gather<GR>(s, L, slot, ft, 0, fast_nvalid(data_bits, U, 0), g);
     front_store_gather<GR>(s, L, ft, 0, g);
     if (nU > 2) wbyte = window_load(t.in, len, U, 2, ft);
@@ -566,7 +593,7 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
     } else {
       if (um >= 0 && um < nU) front_mix(s, L, ft, um, fast_nvalid(data_bits, U, um));
       if (tau + 1 < nU) {
-        front_links(s, L, ft, tau + 1, nv1);
+        front_links<GR / 2>(s, L, ft, tau + 1, nv1);
         if (tau + 2 < nU) {
           if (ft < U / 8 + 7) s.win[ft] = (uint8_t)wbyte;
           front_sync();
