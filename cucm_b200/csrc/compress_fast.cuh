@@ -390,8 +390,11 @@ CUCM_UNROLL
 // Chain (lane = order): StateMap probability updates of unit v in bit order.
 // A record is statep | dt[c] << 32 | dt[c+1] << 48 for the state's count c;
 // the count only ever grows by one per update, so a run of updates of one
-// state needs each table value two steps after it is requested, and the
-// record store is deferred by one step so it never waits for that load.
+// state needs each table value two steps after it is requested.  A step's
+// record is loaded two steps ahead; the two results not yet stored when it
+// was loaded (the previous step's, stored one step late, and the current
+// one) are forwarded from registers, so no shared-memory round trip sits on
+// the step-to-step chain.
 __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &L, int o, int v, int n) {
   const int U = L.U;
   const uint8_t *sta = s.st + (v & 1) * U * kOrders + o;
@@ -400,31 +403,40 @@ __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &
   const uint16_t *dt = s.tab->dt;
   int st = sta[0];
   int st1 = n > 1 ? sta[kOrders] : 0;
+  int st2 = n > 2 ? sta[2 * kOrders] : 0;
   const uint64_t r0 = rec[st * kOrders];
+  uint64_t nraw = rec[st1 * kOrders];
   uint32_t val = (uint32_t)r0, d = (uint32_t)(r0 >> 32) & 0xffffu, dn = (uint32_t)(r0 >> 48);
   int pst = st;
-  uint64_t pnr = r0;
+  uint32_t pv = val, pd = d, pdn = dn;
   uint32_t ywd = 0;
   for (int j = 0; j < n; j++) {
-    rec[pst * kOrders] = pnr;  // deferred store of the previous step
-    const uint64_t r1 = rec[st1 * kOrders];
-    const int st2 = (j + 2 < n) ? sta[(j + 2) * kOrders] : 0;
+    rec[pst * kOrders] = (uint64_t)pv | ((uint64_t)pd << 32) | ((uint64_t)pdn << 48);
+    const uint64_t r2 = rec[st2 * kOrders];
+    const int st3 = (j + 3 < n) ? sta[(j + 3) * kOrders] : 0;
     if ((j & 31) == 0) ywd = yw[j >> 5];
     const uint32_t y = (ywd >> (j & 31)) & 1u;
     const uint32_t cnt = val & 1023u;
     const uint32_t dnn = dt[cnt < 1021u ? cnt + 2 : 1023u];
     const int32_t err = (int32_t)((y << 22) - (val >> 10));
     const uint32_t v2 = val + (((uint32_t)(err >> 3) * d) & 0xfffffc00u) + (cnt < 1023u ? 1u : 0u);
+    const bool f0 = st1 == st, f1 = st1 == pst;
+    const uint32_t nv = f0 ? v2 : f1 ? pv : (uint32_t)nraw;
+    const uint32_t nd = f0 ? dn : f1 ? pd : (uint32_t)(nraw >> 32) & 0xffffu;
+    const uint32_t ndn = f0 ? dnn : f1 ? pdn : (uint32_t)(nraw >> 48);
     pst = st;
-    pnr = (uint64_t)v2 | ((uint64_t)dn << 32) | ((uint64_t)dnn << 48);
-    const bool fwd = st1 == st;
-    val = fwd ? v2 : (uint32_t)r1;
-    d = fwd ? dn : (uint32_t)(r1 >> 32) & 0xffffu;
-    dn = fwd ? dnn : (uint32_t)(r1 >> 48);
+    pv = v2;
+    pd = dn;
+    pdn = dnn;
+    val = nv;
+    d = nd;
+    dn = ndn;
+    nraw = r2;
     st = st1;
     st1 = st2;
+    st2 = st3;
   }
-  rec[pst * kOrders] = pnr;
+  rec[pst * kOrders] = (uint64_t)pv | ((uint64_t)pd << 32) | ((uint64_t)pdn << 48);
 }
 
 // Front: predictions, mixer output and training of unit v; thread t handles
