@@ -187,10 +187,12 @@ __device__ __forceinline__ void front_keys(const FastSmem &s, const FastLayout &
   }
 }
 
-// Slot tables: per order and unit, the unit's distinct keys (key + 1) in
-// ascending order, padded with kNoKey; a key's slot is its rank.  Sorting
-// the unit's keys once replaces a hash table built step by step (a claim
-// loop with a shared-memory round trip and a warp barrier per two bytes).
+// Slot tables: per order and unit, the unit's keys (key + 1) in ascending
+// order, padded with kNoKey; a key's slot is the position of its first
+// occurrence.  Sorting the unit's keys once replaces a hash table built step
+// by step (a claim loop with a shared-memory round trip and a warp barrier
+// per two bytes); keeping the repeats in the row (slots with gaps) saves the
+// compaction.
 constexpr uint32_t kNoKey = 0xffffffffu;
 
 // Ascending bitonic sort of 32 * E values, value p = lane * E + i in a[i]
@@ -227,8 +229,8 @@ __device__ __forceinline__ void warp_sort(uint32_t (&a)[E], int lane) {
   }
 }
 
-// Position of kp in an ascending row of P (a power of two) entries, if it
-// is there: the returned position holds kp exactly when it is present.
+// First position of kp in an ascending row of P (a power of two) entries,
+// if it is there: the returned position holds kp exactly when it is present.
 template <int P>
 __device__ __forceinline__ int row_find(const uint32_t *row, uint32_t kp) {
   int lo = 0;
@@ -240,10 +242,10 @@ __device__ __forceinline__ int row_find(const uint32_t *row, uint32_t kp) {
 // Front: slots of unit v in its own table, and in the previous unit's.
 // Front warp w owns orders 2w and 2w + 1, so no other warp writes their
 // rows.  Per order: the unit's keys (bit j = lane + 32 i) are sorted across
-// the warp, the distinct ones written in order, then every bit finds its
-// key's rank in this unit's row (bkt) and in the previous unit's (lnk =
-// rank + 1, or 0 when the key was not touched there).  E keys per lane:
-// 32 * E >= U, and NSLOT = 32 * E.
+// the warp and written in order, then every bit finds its key's first
+// position in this unit's row (bkt) and in the previous unit's (lnk =
+// position + 1, or 0 when the key was not touched there).  E keys per
+// lane: 32 * E >= U, and NSLOT = 32 * E.
 template <int E>
 __device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
   constexpr int P = 32 * E;
@@ -268,30 +270,8 @@ __device__ __forceinline__ void front_links(const FastSmem &s, const FastLayout 
   CUCM_UNROLL
   for (int h = 0; h < 2; h++) {
     uint32_t *row = s.hk + ((v & 1) * kOrders + 2 * w + h) * P;
-    // distinct keys: a value is the first of its run unless it equals the
-    // one before it (the previous lane's last for i = 0)
-    const uint32_t before = __shfl_up_sync(0xffffffffu, a[h][E - 1], 1);
-    unsigned heads = 0;
     CUCM_UNROLL
-    for (int i = 0; i < E; i++) {
-      const uint32_t prev = i ? a[h][i - 1] : before;
-      if (a[h][i] != kNoKey && (lane * E + i == 0 || a[h][i] != prev)) heads |= 1u << i;
-    }
-    const int cnt = __popc(heads);
-    int incl = cnt;
-    CUCM_UNROLL
-    for (int d = 1; d < 32; d <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, d);
-      if (lane >= d) incl += y;
-    }
-    const int nd = __shfl_sync(0xffffffffu, incl, 31);
-    int at = incl - cnt;
-    CUCM_UNROLL
-    for (int i = 0; i < E; i++) {
-      if (heads >> i & 1u) row[at++] = a[h][i];
-      const int q = lane * E + i;
-      if (q >= nd) row[q] = kNoKey;
-    }
+    for (int i = 0; i < E; i++) row[lane * E + i] = a[h][i];
   }
   __syncwarp();
   CUCM_UNROLL
