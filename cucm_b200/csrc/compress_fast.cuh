@@ -20,7 +20,9 @@
 //     * gathers of unit t+1's slot states from the tables in HBM;
 //     * stretch, mixer context, mixer output and training of unit t-1
 //       (cudamixUnit / cudaupdateMixer, cucm_compress_v2.cu:755-819) against
-//       a snapshot of the probabilities taken when the previous chain ended.
+//       the probabilities as they stand when the previous chain has ended
+//       (read from the StateMap records before the chain of unit t-1
+//       starts on them).
 //   walker warp (2): the bit-history side of the StateMap update for unit
 //     t, in bit order, a byte (64 updates) per step: the state each update
 //     sees (live), the state each prediction saw (frozen = unit-start value),
@@ -40,7 +42,7 @@ constexpr int kFastThreads = kFastWarps * 32;
 constexpr int kFastMaxUnit = 256;
 constexpr int kWChain = 0, kWCoder = 1, kWWalk = 2, kWFront = 3;
 constexpr int kFrontThreads = 128;
-constexpr int kSnapThreads = 32 + kFrontThreads;  // chain + front warps
+constexpr int kSnapThreads = 32 + kFrontThreads;  // chain + front warps (barrier 1)
 constexpr int kWinBytes = kFastMaxUnit / 8 + 8;    // input window of a unit (+7 history bytes)
 
 constexpr int kFastStageMin = 2048;
@@ -52,7 +54,7 @@ typedef Tables FastTables;
 
 struct FastLayout {
   int U, NSLOT, stage;
-  size_t off_tab, off_rec, off_snap, off_w, off_hk, off_ns, off_key, off_lnk, off_bkt, off_fsw, off_st, off_fr,
+  size_t off_tab, off_rec, off_w, off_hk, off_ns, off_key, off_lnk, off_bkt, off_fsw, off_st, off_fr,
       off_yw, off_c1, off_prm, off_win, off_stage, total;
 };
 
@@ -71,7 +73,6 @@ __host__ __device__ inline FastLayout make_fast_layout(int U) {
   };
   L.off_tab = take(sizeof(FastTables));
   L.off_rec = take(sizeof(uint64_t) * kOrders * 256);
-  L.off_snap = take(sizeof(int16_t) * kOrders * 256);
   L.off_w = take(sizeof(int32_t) * kMixCtx * kOrders);
   L.off_hk = take(sizeof(uint32_t) * 2 * kOrders * NS);    // keys + 1 by slot, ascending [unit parity][order][slot]
   L.off_ns = take(sizeof(uint16_t) * 2 * kOrders * NS);    // 0x100 | state once written in the unit
@@ -93,7 +94,6 @@ __host__ __device__ inline FastLayout make_fast_layout(int U) {
 struct FastSmem {
   FastTables *tab;
   uint64_t *rec;     // [256][8]  statep | dt[count] << 32 | dt[count + 1] << 48
-  int16_t *snap;     // [256][8]  stretched probability as of the last finished chain
   int32_t *w;        // [80*8]
   uint32_t *hk;      // [2][8][NSLOT]
   uint16_t *ns;      // [2][8][NSLOT]
@@ -114,7 +114,6 @@ __device__ inline FastSmem carve_fast(uint8_t *b, const FastLayout &L) {
   FastSmem s;
   s.tab = reinterpret_cast<FastTables *>(b + L.off_tab);
   s.rec = reinterpret_cast<uint64_t *>(b + L.off_rec);
-  s.snap = reinterpret_cast<int16_t *>(b + L.off_snap);
   s.w = reinterpret_cast<int32_t *>(b + L.off_w);
   s.hk = reinterpret_cast<uint32_t *>(b + L.off_hk);
   s.ns = reinterpret_cast<uint16_t *>(b + L.off_ns);
@@ -136,7 +135,8 @@ __device__ __forceinline__ void named_barrier(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// Barrier ids: 0 = whole CTA, 1 = chain + front (snapshot), 2 = front only.
+// Barrier ids: 0 = whole CTA, 1 = chain + front (probabilities read before
+// the chain updates them), 2 = front only.
 __device__ __forceinline__ void front_sync() { named_barrier(2, kFrontThreads); }
 
 __device__ __forceinline__ int fast_nvalid(uint64_t data_bits, int U, int v) {
@@ -421,32 +421,46 @@ __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &
   rec[pst * kOrders] = (uint64_t)pv | ((uint64_t)pd << 32) | ((uint64_t)pdn << 48);
 }
 
-// Front: predictions, mixer output and training of unit v; thread t handles
-// bits t and t + 128.
-__device__ __forceinline__ void front_mix(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid) {
+// Front: stretched probabilities of unit v's bits (thread t: bits t and
+// t + 128) as the records stand when the previous chain has ended, read
+// before the chain of unit v changes them.
+__device__ __forceinline__ void front_probs(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid,
+                                            int (&smps)[2][kOrders]) {
   const int U = L.U;
   const uint8_t *fr = s.fr + (v & 1) * U * kOrders;
+  CUCM_UNROLL
+  for (int h = 0; h < 2; h++) {
+    const int j = t + h * kFrontThreads;
+    if (j < U && j < nvalid) {
+      const uint64_t f8 = *reinterpret_cast<const uint64_t *>(fr + j * kOrders);
+      CUCM_UNROLL
+      for (int o = 0; o < kOrders; o++) {
+        const uint32_t stt = (uint32_t)(f8 >> (8 * o)) & 0xffu;
+        smps[h][o] = s.tab->stretch[reinterpret_cast<const uint32_t *>(s.rec)[2 * (stt * kOrders + o)] >> 20];
+      }
+    }
+  }
+}
+
+// Front: predictions, mixer output and training of unit v from the
+// probabilities front_probs read; thread t handles bits t and t + 128.
+__device__ __forceinline__ void front_mix(const FastSmem &s, const FastLayout &L, int t, int v, int nvalid,
+                                          int (&smps)[2][kOrders]) {
+  const int U = L.U;
   const uint32_t *yw = s.yw + (v & 3) * (U / 32);
   const uint8_t *c1 = s.c1 + (v & 3) * (U / 8);
   uint16_t *prm = s.prm + (v & 1) * U;
   const uint16_t *prm_old = s.prm + ((v + 1) & 1) * U;
   int cxs[2] = {0, 0}, errs[2] = {0, 0};
-  int smps[2][kOrders];
   bool has[2] = {false, false};
   CUCM_UNROLL
   for (int h = 0; h < 2; h++) {
     const int j = t + h * kFrontThreads;
     if (j < U) {
       if (j < nvalid) {
-        const uint64_t f8 = *reinterpret_cast<const uint64_t *>(fr + j * kOrders);
         int olen = 0;
         CUCM_UNROLL
-        for (int o = 0; o < kOrders; o++) {
-          const uint32_t stt = (uint32_t)(f8 >> (8 * o)) & 0xffu;
-          const int sm = s.snap[stt * kOrders + o];
-          smps[h][o] = sm;
-          olen += (sm != 1);
-        }
+        for (int o = 0; o < kOrders; o++) olen += (smps[h][o] != 1);
         const int cx = olen + (c1[j >> 3] >> 5) * 10;
         const int pr = mix_pr(s.w, cx, smps[h], s.tab);
         const int y = (yw[j >> 5] >> (j & 31)) & 1;
@@ -566,12 +580,9 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
     // gathers of unit tau+1 go out first; they land while the front works
     const int nv1 = fast_nvalid(data_bits, U, tau + 1);
     if (front && tau + 1 < nU) front_gather<GR>(s, L, slot, ft, tau + 1, nv1, g);
+    int smps[2][kOrders];
     if (warp == kWChain || front) {
-      if (um >= 0 && um < nU) {
-        const int k = warp == kWChain ? lane : 32 + ft;
-        for (int i = k; i < kOrders * 256; i += kSnapThreads)
-          s.snap[i] = s.tab->stretch[(uint32_t)s.rec[i] >> 20];
-      }
+      if (front && um >= 0 && um < nU) front_probs(s, L, ft, um, fast_nvalid(data_bits, U, um), smps);
       named_barrier(1, kSnapThreads);
     }
     if (warp == kWChain) {
@@ -590,7 +601,7 @@ __device__ void compress_fast_one(const ChunkTask &t, uint8_t *slot, const FastS
         walk_unit(s, L, slot, lane, tau, fast_nvalid(data_bits, U, tau));
       }
     } else {
-      if (um >= 0 && um < nU) front_mix(s, L, ft, um, fast_nvalid(data_bits, U, um));
+      if (um >= 0 && um < nU) front_mix(s, L, ft, um, fast_nvalid(data_bits, U, um), smps);
       if (tau + 1 < nU) {
         front_links<GR / 2>(s, L, ft, tau + 1, nv1);
         if (tau + 2 < nU) {
