@@ -80,7 +80,7 @@ __host__ __device__ inline FastLayout make_fast_layout(int U) {
   L.off_lnk = take(sizeof(uint16_t) * 2 * kOrders * U);    // slot + 1 in the previous unit's table, or 0
   L.off_bkt = take(sizeof(uint16_t) * 2 * kOrders * U);    // slot in this unit's table
   L.off_fsw = take((size_t)2 * kOrders * U);               // gathered slot states
-  L.off_st = take((size_t)2 * kOrders * U);                // live state
+  L.off_st = take((size_t)2 * kOrders * U + 4 * kOrders);  // live state (+ the chain's read-ahead)
   L.off_fr = take((size_t)2 * U * kOrders);                // frozen state
   L.off_yw = take(sizeof(uint32_t) * 4 * (U / 32));        // bits, by unit mod 4
   L.off_c1 = take((size_t)4 * (U / 8));                    // previous byte per byte, by unit mod 4
@@ -376,7 +376,9 @@ CUCM_UNROLL
 // record is loaded two steps ahead; the two results not yet stored when it
 // was loaded (the previous step's, stored one step late, and the current
 // one) are forwarded from registers, so no shared-memory round trip sits on
-// the step-to-step chain.
+// the step-to-step chain.  The bits come 32 to a word; the state three
+// steps ahead is read unconditionally (the live-state array has room past
+// its end for it).
 __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &L, int o, int v, int n) {
   const int U = L.U;
   const uint8_t *sta = s.st + (v & 1) * U * kOrders + o;
@@ -391,32 +393,35 @@ __device__ __forceinline__ void fast_chain(const FastSmem &s, const FastLayout &
   uint32_t val = (uint32_t)r0, d = (uint32_t)(r0 >> 32) & 0xffffu, dn = (uint32_t)(r0 >> 48);
   int pst = st;
   uint32_t pv = val, pd = d, pdn = dn;
-  uint32_t ywd = 0;
-  for (int j = 0; j < n; j++) {
-    rec[pst * kOrders] = (uint64_t)pv | ((uint64_t)pd << 32) | ((uint64_t)pdn << 48);
-    const uint64_t r2 = rec[st2 * kOrders];
-    const int st3 = (j + 3 < n) ? sta[(j + 3) * kOrders] : 0;
-    if ((j & 31) == 0) ywd = yw[j >> 5];
-    const uint32_t y = (ywd >> (j & 31)) & 1u;
-    const uint32_t cnt = val & 1023u;
-    const uint32_t dnn = dt[cnt < 1021u ? cnt + 2 : 1023u];
-    const int32_t err = (int32_t)((y << 22) - (val >> 10));
-    const uint32_t v2 = val + (((uint32_t)(err >> 3) * d) & 0xfffffc00u) + (cnt < 1023u ? 1u : 0u);
-    const bool f0 = st1 == st, f1 = st1 == pst;
-    const uint32_t nv = f0 ? v2 : f1 ? pv : (uint32_t)nraw;
-    const uint32_t nd = f0 ? dn : f1 ? pd : (uint32_t)(nraw >> 32) & 0xffffu;
-    const uint32_t ndn = f0 ? dnn : f1 ? pdn : (uint32_t)(nraw >> 48);
-    pst = st;
-    pv = v2;
-    pd = dn;
-    pdn = dnn;
-    val = nv;
-    d = nd;
-    dn = ndn;
-    nraw = r2;
-    st = st1;
-    st1 = st2;
-    st2 = st3;
+  for (int j0 = 0; j0 < n; j0 += 32) {
+    uint32_t ywd = yw[j0 >> 5];
+    const int je = j0 + 32 < n ? j0 + 32 : n;
+    for (int j = j0; j < je; j++) {
+      rec[pst * kOrders] = (uint64_t)pv | ((uint64_t)pd << 32) | ((uint64_t)pdn << 48);
+      const uint64_t r2 = rec[st2 * kOrders];
+      const int st3 = sta[(j + 3) * kOrders];
+      const uint32_t y = ywd & 1u;
+      ywd >>= 1;
+      const uint32_t cnt = val & 1023u;
+      const uint32_t dnn = dt[cnt < 1021u ? cnt + 2 : 1023u];
+      const int32_t err = (int32_t)((y << 22) - (val >> 10));
+      const uint32_t v2 = val + (((uint32_t)(err >> 3) * d) & 0xfffffc00u) + (cnt < 1023u ? 1u : 0u);
+      const bool f0 = st1 == st, f1 = st1 == pst;
+      const uint32_t nv = f0 ? v2 : f1 ? pv : (uint32_t)nraw;
+      const uint32_t nd = f0 ? dn : f1 ? pd : (uint32_t)(nraw >> 32) & 0xffffu;
+      const uint32_t ndn = f0 ? dnn : f1 ? pdn : (uint32_t)(nraw >> 48);
+      pst = st;
+      pv = v2;
+      pd = dn;
+      pdn = dnn;
+      val = nv;
+      d = nd;
+      dn = ndn;
+      nraw = r2;
+      st = st1;
+      st1 = st2;
+      st2 = st3;
+    }
   }
   rec[pst * kOrders] = (uint64_t)pv | ((uint64_t)pd << 32) | ((uint64_t)pdn << 48);
 }
