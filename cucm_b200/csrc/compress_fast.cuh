@@ -12,10 +12,10 @@
 //   front warps (3..6, 128 threads)
 //     * keys of unit t+2 for all 8 orders (one FNV pass per bit,
 //       cucm_compress_v2.cu:723-747), the unit's bits and previous bytes;
-//     * slot links of unit t+1: a shared-memory hash table per order (4-key
-//       buckets, places claimed by warp match and rank) gives every distinct
-//       slot of the unit one place, so every later touch knows it must read
-//       the state its predecessor left; a probe of the previous unit's table
+//     * slot links of unit t+1: per order, the unit's keys sorted across a
+//       warp give every distinct slot of the unit one place (its first
+//       position), so every later touch knows it must read the state its
+//       predecessor left; a binary search of the previous unit's sorted keys
 //       tells whether the slot was touched one unit earlier;
 //     * gathers of unit t+1's slot states from the tables in HBM;
 //     * stretch, mixer context, mixer output and training of unit t-1
