@@ -575,6 +575,8 @@ def main():
         ctx.close()
         del d_in, d_comp, d_dec
         torch.cuda.empty_cache()
+        line["plain_form"] = plain_measure(data)
+        torch.cuda.empty_cache()
         line["batched_vs_plain"] = batch_measure(warmup=1, sample=512)
         torch.cuda.empty_cache()
         line["serve"] = serve_measure([2.0, 8.0, 32.0], args.extra_requests)
@@ -625,6 +627,44 @@ def run_small(args):
                       "compressed_bytes": m, "byte_exact": ok}), flush=True)
     if not ok:
         raise SystemExit("round trip mismatch")
+
+
+def plain_measure(data, reps=1):
+    """The headline buffer (256 MiB mixed, 1 MiB chunks) in the plain form:
+    one single-CTA kernel launch per chunk, on up to 128 streams, as the
+    reference launches per chunk; one untimed warm-up, then `reps` round
+    trips, device time per call; the container is hashed against the
+    reference's."""
+    import hashlib
+    import torch
+    import cucm_b200 as cc
+    n = data.size
+    ctx = cc.Context(0, form=cc.FORM_PLAIN)
+    cap = cc.lib().cucm_compress_bound(n, cc.default_params(**PARAMS))
+    d_in = torch.from_numpy(data).cuda()
+    d_c = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    d_o = torch.empty(n, dtype=torch.uint8, device="cuda")
+    tc = td = 0.0
+    launches = 0
+    for i in range(reps + 1):
+        m = ctx.compress_dev(d_in.data_ptr(), n, d_c.data_ptr(), cap, **PARAMS)
+        sc = ctx.last_stats()
+        ctx.decompress_dev(d_c.data_ptr(), m, d_o.data_ptr(), n)
+        sd = ctx.last_stats()
+        if i:
+            tc += sc["kernel_ms"]
+            td += sd["kernel_ms"]
+            launches = sc["launches"] + sd["launches"]
+    ok = bool(torch.equal(d_o, d_in))
+    got = hashlib.sha256(d_c[:m].cpu().numpy().tobytes()).hexdigest()
+    want = reference_sha256("mixed256M")
+    ctx.close()
+    del d_in, d_c, d_o
+    return {"workload": "the headline buffer, plain form: one single-CTA launch per chunk on up to 128 streams",
+            "compress_MBps": _mbps(n * reps, tc), "decompress_MBps": _mbps(n * reps, td),
+            "round_trip_MBps": _mbps(n * reps, tc + td),
+            "kernel_ms": {"compress": tc / reps, "decompress": td / reps}, "launches_per_round_trip": launches,
+            "sha256_match": (got == want) if want else None, "byte_exact": ok}
 
 
 def batch_measure(warmup=1, sample=512):
