@@ -447,10 +447,10 @@ def main():
         sample = data[:32 << 20]
         best, cands = ctx.autotune(sample, reps=1, chunksize=max(sample.size // max(nch, 1), 4096),
                                    unit=PARAMS["unit"], batch=PARAMS["batch"])
-        tuned = {"chosen": {k: best[k] for k in ("form", "dec_pairs", "dec_tables")},
+        keys = ("form", "kernel", "cmp_ctas", "dec_pairs", "dec_tables")
+        tuned = {"chosen": {k: best[k] for k in keys},
                  "sample": "first 32 MiB, %d chunks" % nch,
-                 "candidates": [{k: c[k] for k in ("form", "dec_pairs", "dec_tables", "compress_ms",
-                                                   "decompress_ms")} for c in cands]}
+                 "candidates": [{k: c[k] for k in keys + ("compress_ms", "decompress_ms")} for c in cands]}
     p = cc.default_params(**PARAMS)
     cap = cc.lib().cucm_compress_bound(n, p)
     d_in = torch.from_numpy(data).to(dev)

@@ -1,8 +1,10 @@
 // autotune.cu -- measured choice of the execution form (cucm_autotune).
 //
-// The reference fixes its launch shapes; here the launch form, the decoder's
-// chunks per CTA and its order 0/1 table placement are execution choices
-// that never change an output byte.  The autotuner runs every candidate
+// The reference fixes its launch shapes; here the launch form, the
+// compressor's CTAs per SM, the warps per chunk (the pipelined kernels: 7
+// warps per chunk to compress, a pair to decode; the generic kernels: 8
+// warps per chunk), the decoder's chunks per CTA and its order 0/1 table
+// placement are execution choices that never change an output byte.  The autotuner runs every candidate
 // through the public entry points on the caller's sample, checks that all of
 // them give the same container and give the sample back, and applies the
 // one with the least compress + decompress device time.
@@ -66,6 +68,7 @@ extern "C" int cucm_autotune(cucm_ctx *c, const uint8_t *sample, uint64_t n, con
     cucm_tune_result r;
     r.tuning = base;
     r.tuning.form = form;
+    r.tuning.kernel = 0;
     r.tuning.dec_pairs = 0;
     r.tuning.dec_tables = 0;
     r.tuning.cmp_ctas = 0;
@@ -100,6 +103,16 @@ extern "C" int cucm_autotune(cucm_ctx *c, const uint8_t *sample, uint64_t n, con
       cands.push_back(r);
     }
   }
+  {
+    // the generic kernel (8 warps per chunk), persistent form
+    cucm_tune_result r = candidate(CUCM_FORM_PERSISTENT);
+    r.tuning.kernel = 1;
+    cucm_ctx_set_tuning(c, &r.tuning);
+    rc = timed_compress(c, sample, n, p, reps, out, r.compress_ms);
+    if (rc) return fail(rc);
+    if (out != ref) return fail(CUCM_EMISMATCH);
+    cands.push_back(r);
+  }
   // decoder: chunks per CTA and table placement in the persistent form
   for (int f = 0; f < 2; f++) {
     const int max_pairs = forms[f] == CUCM_FORM_PERSISTENT ? 5 : 0;
@@ -115,22 +128,33 @@ extern "C" int cucm_autotune(cucm_ctx *c, const uint8_t *sample, uint64_t n, con
       }
     }
   }
+  {
+    cucm_tune_result r = candidate(CUCM_FORM_PERSISTENT);
+    r.tuning.kernel = 1;
+    cucm_ctx_set_tuning(c, &r.tuning);
+    rc = timed_decompress(c, ref, sample, n, reps, back, r.decompress_ms);
+    if (rc) return fail(rc);
+    cands.push_back(r);
+  }
 
-  // per form, the fastest compressor and the fastest decoder choice; the form
-  // with the least sum wins
+  // per form and kernel, the fastest compressor and the fastest decoder
+  // choice; the pair with the least sum wins
   double best_total = -1.0;
   for (int f = 0; f < 2; f++) {
-    const cucm_tune_result *bc = nullptr, *bd = nullptr;
-    for (const cucm_tune_result &r : cands) {
-      if (r.tuning.form != forms[f]) continue;
-      if (r.compress_ms >= 0.0 && (!bc || r.compress_ms < bc->compress_ms)) bc = &r;
-      if (r.decompress_ms >= 0.0 && (!bd || r.decompress_ms < bd->decompress_ms)) bd = &r;
-    }
-    const double total = bc->compress_ms + bd->decompress_ms;
-    if (best_total < 0.0 || total < best_total) {
-      best_total = total;
-      *best = bd->tuning;
-      best->cmp_ctas = bc->tuning.cmp_ctas;
+    for (int kern = 0; kern < 2; kern++) {
+      const cucm_tune_result *bc = nullptr, *bd = nullptr;
+      for (const cucm_tune_result &r : cands) {
+        if (r.tuning.form != forms[f] || r.tuning.kernel != kern) continue;
+        if (r.compress_ms >= 0.0 && (!bc || r.compress_ms < bc->compress_ms)) bc = &r;
+        if (r.decompress_ms >= 0.0 && (!bd || r.decompress_ms < bd->decompress_ms)) bd = &r;
+      }
+      if (!bc || !bd) continue;
+      const double total = bc->compress_ms + bd->decompress_ms;
+      if (best_total < 0.0 || total < best_total) {
+        best_total = total;
+        *best = bd->tuning;
+        best->cmp_ctas = bc->tuning.cmp_ctas;
+      }
     }
   }
   cucm_ctx_set_tuning(c, best);

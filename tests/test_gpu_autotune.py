@@ -1,6 +1,7 @@
 """The measured autotuner (cucm_autotune): every execution choice it tries
 must give the same container and give the sample back, and the choice it
 applies is the fastest it measured.  The knobs it turns -- launch form,
+compressor CTAs per SM, warps per chunk (pipelined or generic kernels),
 decoder chunks per CTA, order 0/1 table placement -- never change a byte."""
 import pytest
 
@@ -23,17 +24,26 @@ def test_autotune_measures_every_choice_and_applies_the_fastest(ctx, oracle_mod)
     best, cands = ctx.autotune(sample, reps=1, chunksize=16384)
     comp_c = [c for c in cands if c["compress_ms"] >= 0]
     dec_c = [c for c in cands if c["decompress_ms"] >= 0]
-    # compressor: persistent with 1 or 2 CTAs per SM, plain; decoder:
-    # persistent with 0..5 chunks per CTA x 2 table placements, plain x 2
-    assert (len(comp_c), len(dec_c)) == (3, 14)
+    # compressor: persistent with 1 or 2 CTAs per SM, plain, persistent
+    # generic (8 warps per chunk); decoder: persistent with 0..5 chunks per
+    # CTA x 2 table placements, plain x 2, persistent generic
+    assert (len(comp_c), len(dec_c)) == (4, 15)
+    assert sum(c["kernel"] == 1 for c in comp_c) == 1 and sum(c["kernel"] == 1 for c in dec_c) == 1
     assert all(c["compress_ms"] > 0 for c in comp_c) and all(c["decompress_ms"] > 0 for c in dec_c)
     totals = {}
     for form in (cc.FORM_PERSISTENT, cc.FORM_PLAIN):
-        bc = min((c for c in comp_c if c["form"] == form), key=lambda c: c["compress_ms"])
-        bd = min((c for c in dec_c if c["form"] == form), key=lambda c: c["decompress_ms"])
-        totals[form] = (bc["compress_ms"] + bd["decompress_ms"], bc["cmp_ctas"], bd["dec_pairs"], bd["dec_tables"])
-    form = min(totals, key=lambda f: totals[f][0])
-    assert (best["form"], best["cmp_ctas"], best["dec_pairs"], best["dec_tables"]) == (form,) + totals[form][1:]
+        for kern in (0, 1):
+            cs = [c for c in comp_c if c["form"] == form and c["kernel"] == kern]
+            ds = [c for c in dec_c if c["form"] == form and c["kernel"] == kern]
+            if not cs or not ds:
+                continue
+            bc = min(cs, key=lambda c: c["compress_ms"])
+            bd = min(ds, key=lambda c: c["decompress_ms"])
+            totals[(form, kern)] = (bc["compress_ms"] + bd["decompress_ms"], bc["cmp_ctas"], bd["dec_pairs"],
+                                    bd["dec_tables"])
+    form, kern = min(totals, key=lambda f: totals[f][0])
+    assert ((best["form"], best["kernel"], best["cmp_ctas"], best["dec_pairs"], best["dec_tables"])
+            == (form, kern) + totals[(form, kern)][1:])
     assert ctx.get_tuning() == best
     comp = ctx.compress(sample, chunksize=16384)
     assert comp == want
