@@ -56,6 +56,8 @@ CASES = [
     ("walk", 200000, 32768, 128, 0, 3),
     ("runs", 150000, 65536, 64, 0, 100),
     ("random", 70000, 16384, 256, 0, 2),
+    ("text", 60000, 16384, 160, 0, 100),      # units of 160..224 bits: 8 keys per lane, padded
+    ("walk", 50000, 8192, 224, 0, 5),
     ("text", 100000, 10000, 96, 20000, 100),
     ("text", 65536 * 3, 65536, 128, 0, 1),
     ("walk", 12345, 1000, 32, 0, 7),
