@@ -263,14 +263,13 @@ int cucm_last_device_ms(cucm_ctx *ctx, double *ms);
 /* Number of kernels this context launched in the last call. */
 int cucm_last_launches(cucm_ctx *ctx, uint64_t *n);
 
-/* Figures of the last call: device_ms as above, kernel_ms the time of the
- * coder kernels alone (CUDA events around their launches), launches, and
- * the number of chunks coded. */
 /* Measured autotuner.  No counterpart in the reference, whose launch
  * shapes are fixed.  Codes `sample` (host memory, n bytes) with `p` under
  * every candidate execution choice -- launch form; for the persistent
  * compressor, CTAs per SM (1, 2); for the persistent decoder, chunks per
- * CTA (0..5) and order 0/1 table placement -- `reps`
+ * CTA (0..5) and order 0/1 table placement; in the persistent form, warps
+ * per chunk (the pipelined kernels, kernel = 0, or the generic ones,
+ * kernel = 1) -- `reps`
  * times each (>= 1; the fastest repetition counts), checks that every
  * candidate gives the same container and gives the sample back (else
  * CUCM_EMISMATCH), then applies to the context and writes to *best the
@@ -286,6 +285,9 @@ typedef struct cucm_tune_result {
 int cucm_autotune(cucm_ctx *ctx, const uint8_t *sample, uint64_t n, const cucm_params *p, int reps,
                   cucm_tune_result *results, uint32_t cap, uint32_t *count, cucm_tuning *best);
 
+/* Figures of the last call: device_ms as above, kernel_ms the time of the
+ * coder kernels alone (CUDA events around their launches), launches, and
+ * the number of chunks coded. */
 typedef struct cucm_stats {
   double device_ms;
   double kernel_ms;
